@@ -1,0 +1,339 @@
+"""Benchmark of the B200 per-stage DG update for 2D ideal MHD.
+
+Metric: FP64 DOF-stage updates per second (DOF = element x GLL node x conserved variable; one
+SSP-RK3 time step = 3 stage updates of every DOF).  Workload (default): the smooth isentropic MHD
+vortex on [-10,10]^2, periodic, 512x512 elements, degree 3 (16 GLL nodes per element, 33.5 M DOFs),
+gamma = 5/3, SSP-RK3, CFL 0.6, OEDG + LDF + positivity limiter on -- the largest single-GPU
+configuration of the vortex convergence study.  Synthetic input: the analytic initial condition.
+
+Legs in one JSON line:
+  value     device-resident time steps (mhd_gpu_advance), state resident in HBM;
+  e2e       the same steps through the C ABI with host buffers: per step the Fortran-layout state is
+            uploaded from pinned host memory, one step runs, and the state is downloaded;
+  roofline  the dominant kernel (the DG residual) timed live with CUDA events on the solver's stream;
+  cpu_baseline  the CPU oracle (OpenMP, all host threads) on a bounded sample of the same workload.
+Multi-GPU: replicas only (independent instances, no exchange); value = sum over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (problem, n, p, use_oedg, use_ldf)
+    "vortex512_p3": ("vortex", 512, 3, True, True),
+    "vortex256_p3": ("vortex", 256, 3, True, True),
+    "blast400_p2": ("blast", 400, 2, True, True),
+    "ot64_p2": ("ot2pi", 64, 2, True, True),
+}
+KERNELS_PER_TRY_RK3 = 34  # kernel nodes of one captured try (see enqueue_try in mhd_gpu.cu)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------ clocks sampling
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------ distributed
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1, 0
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist, rank, ws, local
+
+
+def max_over_ranks(dist, x, device=None):
+    """max of a scalar over all ranks (the multi-GPU timing rule)"""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ------------------------------------------------------------------------------ CPU legs
+def cpu_sample(prob_name, n, p, use_oedg, use_ldf, budget_s=15.0, max_steps=50, threads=None):
+    """time whole SSP-RK3 steps of the oracle (fast build, OpenMP) on the workload mesh"""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    from oracle import oracle as ora
+    prob = pkg.problems.make(prob_name)
+    u0 = prob.initial_state(n, n, p)
+    nthreads = threads or os.cpu_count()
+    o = ora.OracleSolver(n, n, p, p, 3, *prob.domain, prob.gamma, prob.bc_kind, prob.bc_state,
+                         fast=True, threads=nthreads)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    o.solve(prob.final_T, prob.cfl, use_oedg, use_ldf, max_steps=1)  # prologue + 1 warm step
+    t0 = time.perf_counter()
+    o.solve(prob.final_T, prob.cfl, use_oedg, use_ldf, max_steps=1, resume=True)
+    t1 = time.perf_counter() - t0
+    k = max(1, min(max_steps, int(budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    o.solve(prob.final_T, prob.cfl, use_oedg, use_ldf, max_steps=k, resume=True)
+    el = time.perf_counter() - t0
+    dofs = 8 * n * n * (p + 1) ** 2
+    o.close()
+    return {"value": 3 * dofs * k / el, "unit": "DOF-stage/s", "cores": nthreads,
+            "kind": "port", "sample": f"{k} SSP-RK3 steps of the full {n}x{n} p={p} mesh "
+                                      f"(oracle -O3 -march=native, OpenMP {nthreads} threads)",
+            "seconds": el}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference's path (no Fortran compiler here)."""
+    if int(os.environ.get("RANK", "0")) != 0:  # under torchrun only rank 0 times the CPU path
+        return
+    prob_name, n, p, oedg, ldf = WORKLOADS[args.workload]
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    from oracle import oracle as ora
+    prob = pkg.problems.make(prob_name)
+    u0 = prob.initial_state(n, n, p)
+    nthreads = os.cpu_count()
+    o = ora.OracleSolver(n, n, p, p, 3, *prob.domain, prob.gamma, prob.bc_kind, prob.bc_state,
+                         fast=True, threads=nthreads)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    o.solve(prob.final_T, prob.cfl, oedg, ldf, max_steps=1)
+    for _ in range(args.warmup):
+        o.solve(prob.final_T, prob.cfl, oedg, ldf, max_steps=1, resume=True)
+    t0 = time.perf_counter()
+    o.solve(prob.final_T, prob.cfl, oedg, ldf, max_steps=args.steps, resume=True)
+    el = time.perf_counter() - t0
+    dofs = 8 * n * n * (p + 1) ** 2
+    val = 3 * dofs * args.steps / el
+    line = {
+        "impl": "reference", "metric": "FP64 DOF-stage updates/s", "value": val, "unit": "DOF-stage/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic initial condition)",
+        "config": {"workload": args.workload, "mesh": f"{n}x{n}", "degree": p, "rk": "SSP-RK3",
+                   "oedg": oedg, "ldf": ldf, "pp": True},
+        "cpu_baseline": {"value": val, "unit": "DOF-stage/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{args.steps} SSP-RK3 steps of the full mesh per timed run "
+                                   "(C restatement of the reference, -O3 -march=native, OpenMP; the "
+                                   "Fortran reference cannot be compiled: no Fortran compiler)"},
+        "e2e": {"value": val, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------ GPU leg
+def run_ours(args):
+    import torch
+    dist, rank, ws, local = dist_setup()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    prob_name, n, p, oedg, ldf = WORKLOADS[args.workload]
+    prob = pkg.problems.make(prob_name)
+    u0 = prob.initial_state(n, n, p)
+    dofs = 8 * n * n * (p + 1) ** 2
+    stream = torch.cuda.Stream(device=device)
+    solver = pkg.DGSolver.for_problem(prob, n, n, p)
+    solver.set_stream(stream.cuda_stream)
+    solver.upload_state(0, u0)
+    solver.solve_begin(prob.final_T, prob.cfl, oedg, ldf, False)
+
+    # ---- value: device-resident steps ----
+    # clocks are sampled from the start of the warm-up (already under load) to the end of the
+    # timed region
+    sampler = ClockSampler(device.index)
+    sampler.start()
+    solver.advance(args.warmup)
+    st0 = solver.status()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    st_run = solver.advance(args.steps, check_every=max(1, args.steps))
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize(device)
+    barrier(dist, device)
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    tries = st_run["steps"] - st0["steps"] + st_run["retries"] - st0["retries"]
+    ms_max = max_over_ranks(dist, ms, device)
+    steps_done = st_run["steps"] - st0["steps"]
+
+    # ---- roofline: the residual kernel timed alone on the same stream ----
+    nrep = 20
+    solver.semidiscretize(1, 0)
+    ek0, ek1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    with torch.cuda.stream(stream):
+        ek0.record(stream)
+    lib = solver.lib
+    for _ in range(nrep):
+        lib.mhd_gpu_semidiscretize(solver.h, 1, 0, None)
+    with torch.cuda.stream(stream):
+        ek1.record(stream)
+    torch.cuda.synchronize(device)
+    t_res = ek0.elapsed_time(ek1) / nrep * 1e-3
+    nodes = n * n * (p + 1) ** 2
+    res_bytes = 2 * 64 * nodes  # read u (8 doubles/node) + write ut (8 doubles/node)
+    hbm_peak, peak_kind = peaks()
+    achieved = res_bytes / t_res / 1e9
+
+    # ---- e2e: host buffers through the C ABI, per step upload + step + download ----
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(u0.size, dtype=torch.float64, pin_memory=True)
+        host_np = host.numpy().reshape(u0.shape, order="F")
+        host_np[...] = u0
+        out = torch.empty(u0.size, dtype=torch.float64, pin_memory=True)
+        out_np = out.numpy().reshape(u0.shape, order="F")
+        k_e2e = max(1, min(args.steps, 5))
+        solver.upload_state(0, host_np)
+        solver.solve_begin(prob.final_T, prob.cfl, oedg, ldf, False)
+        solver.step()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            solver.upload_state(0, host_np)
+            solver.step()
+            solver.download_state(0, out_np)
+        el = time.perf_counter() - t0
+        el = max_over_ranks(dist, el, device)
+        e2e = {"value": 3 * dofs * k_e2e * ws / el, "unit": "DOF-stage/s",
+               "h2d_bytes_per_step": int(u0.nbytes), "d2h_bytes_per_step": int(u0.nbytes) + 64,
+               "steps": k_e2e, "ms_per_step": 1e3 * el / k_e2e}
+
+    line = None
+    if rank == 0:
+        value = 3 * dofs * steps_done * ws / (ms_max * 1e-3)
+        line = {
+            "metric": "FP64 DOF-stage updates/s", "value": value, "unit": "DOF-stage/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / max(1, steps_done), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic initial condition)",
+            "config": {"workload": args.workload, "problem": prob_name, "mesh": f"{n}x{n}",
+                       "degree": p, "dofs": dofs, "rk": "SSP-RK3", "cfl": prob.cfl, "oedg": oedg,
+                       "ldf": ldf, "pp": True, "parallelism": f"replicas{ws}",
+                       "l2": "inputs larger than L2 (state %.0f MB per stage buffer)" % (u0.nbytes / 1e6),
+                       "tries": tries},
+            "gpu_launches": KERNELS_PER_TRY_RK3 * tries,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None, "kernel": "residual_kernel",
+                         "algorithmic_bytes_per_launch": res_bytes, "launch_ms": t_res * 1e3,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "clocks": clocks,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if not args.no_cpu and ws == 1:
+            line["cpu_baseline"] = cpu_sample(prob_name, n, p, oedg, ldf, budget_s=args.cpu_budget)
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist:
+        barrier(dist, device)
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="vortex512_p3", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/*
+ * mhd_gpu.h -- C ABI of the B200 (sm_100a) per-stage DG update for 2D ideal MHD.
+ *
+ * This is the drop-in boundary for the reference YueWu2002/PP-ES-DG-MHD.  The reference's
+ * Fortran driver (drive.f90), set-ups (problems.f90) and output (io.f90) call the hot path
+ * through Fortran module procedures and module-level arrays (DG_solver.f90:6-43).  Each entry
+ * point below replaces one of those procedures; a Fortran caller binds them with
+ * ISO_C_BINDING (interface blocks with bind(C), type(c_ptr), value handles).
+ *
+ * Conventions
+ *   - Every function returns int: 0 = OK, > 0 = sticky solver flag bits (MHD_FLAG_*),
+ *     < 0 = API error (MHD_ERR_*).  Nothing aborts the process (the reference's
+ *     `error stop` conditions become flags).
+ *   - All arrays are FP64 in the reference's Fortran (column-major) layouts:
+ *         u      (8, px+1, py+1, 0:nx+1, 0:ny+1)   state with one ghost layer
+ *         ut     (8, px+1, py+1, nx, ny)           time derivative
+ *         u_avg  (8, 0:nx+1, 0:ny+1)               cell averages
+ *         xx     (px+1, nx),  yy (py+1, ny)        GLL node coordinates
+ *     The library keeps its own element-blocked device layout and transposes on the GPU at
+ *     upload/download.  Host pointers may be pageable or pinned (pinned is faster).
+ *   - One handle is used by one host thread at a time.  Handles are independent (no
+ *     module-level state), so many solver instances may coexist in one process.
+ *   - Supported: px == py in {1,2,3}; rknstg in {1,2,3,5}; nx, ny >= 2.
+ */
+#ifndef MHD_GPU_H
+#define MHD_GPU_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mhd_gpu mhd_gpu_t;
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define MHD_OK 0
+#define MHD_FLAG_NEG_AVG 1        /* inadmissible cell average (DG_solver.f90:189-193)       */
+#define MHD_FLAG_PP_RELIMIT 2     /* PP re-limit failed (DG_solver.f90:582-586, error stop)  */
+#define MHD_FLAG_DT_COLLAPSE 4    /* dt collapse / too many retries (drive.f90:97-100)       */
+#define MHD_FLAG_INIT_NEG_AVG 8   /* initial value inadmissible (drive.f90:70)               */
+#define MHD_ERR_INVALID -1        /* bad argument                                            */
+#define MHD_ERR_UNSUPPORTED -2    /* configuration not supported by the kernels              */
+#define MHD_ERR_CUDA -3           /* a CUDA runtime call failed                              */
+#define MHD_ERR_NO_DEVICE -4      /* no CUDA device visible                                  */
+#define MHD_ERR_STATE -5          /* call out of order (e.g. step before solve_begin)        */
+
+/* ---- boundary-condition kinds (replace the BC_handle procedure pointer, drive.f90:25) --- */
+#define MHD_BC_PERIODIC 0         /* BC_periodic     problems.f90:312-348 */
+#define MHD_BC_EXTRAPOLATE 1      /* BC_YeeSjogreen  problems.f90:386-423 (outflow) */
+#define MHD_BC_FIXED 2            /* BC_rotor        problems.f90:597-654 (bc_state8 = conserved state) */
+#define MHD_BC_XEXTRAP_YPER 3     /* BC_BrioWu       problems.f90:350-384 */
+
+/* status of the device-resident driver (the scalars solve_execute keeps, drive.f90:39-48) */
+typedef struct mhd_gpu_status {
+  double t;            /* simulated time after the last accepted step              */
+  double dt;           /* dt of the last try                                        */
+  double dt_lim;       /* dt limit of the last residual (DG_semidiscretize out)     */
+  double tot_ent;      /* total entropy of the last final stage                     */
+  long long steps;     /* accepted time steps                                       */
+  long long retries;   /* re-tries (drive.f90:102)                                  */
+  long long num_negcell_total; /* PP-limited cells summed over all accepted stages  */
+  int num_negcell_last;/* PP-limited cells of the last stage                        */
+  int done;            /* t reached final_T                                         */
+  int flags;           /* MHD_FLAG_* bits                                           */
+  int pad_;
+} mhd_gpu_status;
+
+/* ---- life cycle ------------------------------------------------------------------------- */
+
+/* init_DG_solver(nx,ny,px,py,rknstg,l,r,b,t) (DG_solver.f90:47-107) + set_gamma (MHD_PDE.f90:5)
+ * + the choice of BC_handle (drive.f90:25).  Allocates every device array NaN-filled
+ * (DG_solver.f90:56,68-85).  bc_state8 is required for MHD_BC_FIXED, else may be NULL. */
+int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, double right,
+                   double bottom, double top, double gamma, int bc_kind, const double *bc_state8,
+                   mhd_gpu_t **out);
+
+/* finalize_DG_solver (DG_solver.f90:109-123) */
+int mhd_gpu_destroy(mhd_gpu_t *h);
+
+/* Run all later work of this handle on the given cudaStream_t (NULL = the handle's own). */
+int mhd_gpu_set_stream(mhd_gpu_t *h, void *cuda_stream);
+
+/* Device bytes held by this handle (state, stages, scratch); no reference counterpart —
+ * used by a caller that admits many solver instances into a fixed HBM budget. */
+int mhd_gpu_device_bytes(const mhd_gpu_t *h, size_t *bytes);
+
+/* Block the host until all work queued on the handle's stream is finished. */
+int mhd_gpu_synchronize(mhd_gpu_t *h);
+
+/* Human-readable text of a status code. */
+const char *mhd_gpu_status_string(int code);
+
+/* ---- geometry and tables ---------------------------------------------------------------- */
+
+/* module variables xx(px+1,nx), yy(py+1,ny) (DG_solver.f90:24,101-106): the node
+ * coordinates that Init_type callbacks receive (drive.f90:6-12). */
+int mhd_gpu_nodes(const mhd_gpu_t *h, double *xx, double *yy);
+
+/* gauss_lobatto (gauss.f90:17-71) + gauss_lobatto_matrix (gauss.f90:134-331) for degree p<=6:
+ * x,w (p+1); M, Minv, D, Pmn, Pnm ((p+1)x(p+1), column-major).  Any pointer may be NULL. */
+int mhd_gpu_gll_tables(int p, double *x, double *w, double *M, double *Minv, double *D,
+                       double *Pmn, double *Pnm);
+
+/* The locally divergence-free projection that post_process applies to (Bx,By) on an hx x hy
+ * element of degree p (DG_solver.f90:231-266 with LDF.f90:114-250), folded into one dense nodal
+ * operator A of size (2n^2)x(2n^2), n = p+1, column-major:
+ *     [Bx;By]_new - avg = A ([Bx;By] - avg),   node index k + n*l, Bx block first.
+ * Host-only (no GPU needed); the kernels apply exactly this matrix.  p in 1..6. */
+int mhd_gpu_ldf_operator(int p, double hx, double hy, double *A);
+
+/* ---- state transfer (Fortran layouts) --------------------------------------------------- */
+
+/* slot 0 = u_con, slot s in 1..rknstg = uRK_con(:,:,:,:,:,s) (DG_solver.f90:12,14) */
+int mhd_gpu_upload_state(mhd_gpu_t *h, int slot, const double *u);
+int mhd_gpu_download_state(mhd_gpu_t *h, int slot, double *u);
+/* ut_con(:,:,:,:,:,stage), stage in 1..rknstg (DG_solver.f90:13) */
+int mhd_gpu_upload_ut(mhd_gpu_t *h, int stage, const double *ut);
+int mhd_gpu_download_ut(mhd_gpu_t *h, int stage, double *ut);
+/* u_avg (DG_solver.f90:11), the input of save_tecbin_finite_volume (io.f90:4) */
+int mhd_gpu_download_avg(mhd_gpu_t *h, double *u_avg);
+
+/* ---- the reference's per-call interface -------------------------------------------------- */
+
+/* BC_handle(u_con or uRK_con(:,s), ...) (drive.f90:68,71,277,291) */
+int mhd_gpu_apply_bc(mhd_gpu_t *h, int slot);
+
+/* post_process(u, u_avg, neg_avg, num_negcell, apply_oedg, apply_LDF, oedg_dt, ent_offset,
+ *              comput_ent, tot_ent) (DG_solver.f90:128-661) on state slot `slot`.
+ * neg_avg/num_negcell/tot_ent may be NULL.  Returns MHD_FLAG_PP_RELIMIT where the reference
+ * would `error stop 123456789`. */
+int mhd_gpu_post_process(mhd_gpu_t *h, int slot, int apply_oedg, int apply_ldf, double oedg_dt,
+                         int ent_offset, int comput_ent, int *neg_avg, int *num_negcell,
+                         double *tot_ent);
+
+/* DG_semidiscretize(ut_con(:,:,:,:,:,ut_stage), dt_lim, u) (DG_solver.f90:663-892) where u is
+ * state slot `slot`.  dt_lim may be NULL. */
+int mhd_gpu_semidiscretize(mhd_gpu_t *h, int ut_stage, int slot, double *dt_lim);
+
+/* The convex stage update of stage `stage` of SSP-RK(rknstg) with step dt
+ * (drive.f90:130-275): writes the interior of uRK_con(:,stage). */
+int mhd_gpu_rk_combine(mhd_gpu_t *h, int stage, double dt);
+
+/* ---- device-resident solve_execute (drive.f90:32-343) ----------------------------------- */
+
+/* Prologue of solve_execute after Init_handle filled u_con (drive.f90:67-75): BC,
+ * post_process (no OEDG, comput_ent), BC, DG_semidiscretize(ut(:,1)).  Also records
+ * final_T, CFL and the limiter switches for the following steps.  tot_ent/dt_lim may be NULL. */
+int mhd_gpu_solve_begin(mhd_gpu_t *h, double final_T, double cfl, int use_oedg, int use_ldf,
+                        int ent_offset, double *tot_ent, double *dt_lim);
+
+/* One time step of the solving loop (drive.f90:83-320) including its re-tries, entirely on the
+ * device; blocks until the step is done and fills *st (may be NULL). */
+int mhd_gpu_step(mhd_gpu_t *h, mhd_gpu_status *st);
+
+/* Up to max_steps time steps (<= 0: until final_T), queued without host round trips;
+ * the host checks progress every `check_every` steps (<= 0: a default). */
+int mhd_gpu_advance(mhd_gpu_t *h, long long max_steps, int check_every, mhd_gpu_status *st);
+
+/* Current driver status without advancing. */
+int mhd_gpu_get_status(mhd_gpu_t *h, mhd_gpu_status *st);
+
+/* Device address of a state slot in the library's element-blocked layout
+ * [ (ny+2) rows ][ (nx+2) elements ][ 8 variables ][ (px+1)*(py+1) nodes ]  (for callers that
+ * keep data on the GPU, e.g. a PyTorch tensor view).  No reference counterpart. */
+int mhd_gpu_state_device_ptr(mhd_gpu_t *h, int slot, double **dptr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

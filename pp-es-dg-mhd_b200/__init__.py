@@ -1,0 +1,215 @@
+"""pp_es_dg_mhd_b200 -- B200 (sm_100a) per-stage DG update for 2D ideal MHD.
+
+Host-side mirror of the reference's solver interface (YueWu2002/PP-ES-DG-MHD), over the C ABI of
+include/mhd_gpu.h:
+
+    reference (Fortran)                                   here
+    init_DG_solver(nx,ny,px,py,rknstg,l,r,b,t)            DGSolver(nx, ny, p, rknstg, domain, gamma, bc)
+      DG_solver.f90:47
+    post_process(u, u_avg, neg_avg, num_negcell, ...)     DGSolver.post_process(slot, ...)
+      DG_solver.f90:128
+    DG_semidiscretize(ut(:,s), dt_lim, u)                 DGSolver.semidiscretize(stage, slot)
+      DG_solver.f90:663
+    BC_handle(u, ...)            drive.f90:25             DGSolver.apply_bc(slot)
+    stage update                 drive.f90:130-275        DGSolver.rk_combine(stage, dt)
+    solve_execute(final_T, CFL, use_oedg, use_LDF,        DGSolver.solve_execute(...)
+                  ent_offset)    drive.f90:32
+    finalize_DG_solver           DG_solver.f90:109        DGSolver.close()
+
+State arrays cross the boundary in the reference's Fortran layouts (numpy, order='F').
+The reference stops the program (`error stop`) on fatal conditions; here those raise MHDError.
+All compute runs in the CUDA library; there is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi, problems
+from .capi import (BC_EXTRAPOLATE, BC_FIXED, BC_PERIODIC, BC_XEXTRAP_YPER, MHDError, Status)
+
+__all__ = ["DGSolver", "MHDError", "capi", "problems", "BC_PERIODIC", "BC_EXTRAPOLATE",
+           "BC_FIXED", "BC_XEXTRAP_YPER", "library_path", "ldf_operator"]
+
+_dp = C.POINTER(C.c_double)
+
+
+def library_path():
+    return capi.LIB_PATH
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def ldf_operator(p, hx, hy):
+    """Dense nodal LDF operator of the library (host-only, no GPU needed)."""
+    n2 = 2 * (p + 1) ** 2
+    A = np.zeros((n2, n2), order="F")
+    rc = capi.load().mhd_gpu_ldf_operator(int(p), float(hx), float(hy), _p(A))
+    if rc:
+        raise MHDError("mhd_gpu_ldf_operator", rc)
+    return A
+
+
+def _check(fn, rc, fatal_flags=True):
+    if rc < 0 or (fatal_flags and rc & (capi.MHD_FLAG_PP_RELIMIT | capi.MHD_FLAG_DT_COLLAPSE |
+                                        capi.MHD_FLAG_INIT_NEG_AVG)):
+        raise MHDError(fn, rc)
+    return rc
+
+
+class DGSolver:
+    """One solver instance (the reference's DG_solver_m module state, but per object)."""
+
+    def __init__(self, nx, ny, p, rknstg=3, domain=(0.0, 1.0, 0.0, 1.0), gamma=5.0 / 3.0,
+                 bc_kind=BC_PERIODIC, bc_state=None):
+        self.lib = capi.load()
+        self.nx, self.ny, self.p, self.rknstg = nx, ny, p, rknstg
+        self.domain, self.gamma, self.bc_kind = tuple(domain), gamma, bc_kind
+        n = p + 1
+        self.shape_u = (8, n, n, nx + 2, ny + 2)
+        self.shape_ut = (8, n, n, nx, ny)
+        self.shape_avg = (8, nx + 2, ny + 2)
+        st = None
+        if bc_state is not None:
+            self._bc = np.ascontiguousarray(bc_state, dtype=np.float64)
+            st = _p(self._bc)
+        h = C.c_void_p()
+        rc = self.lib.mhd_gpu_create(nx, ny, p, p, rknstg, *map(float, domain), float(gamma), bc_kind,
+                                     st, C.byref(h))
+        _check("mhd_gpu_create", rc)
+        self.h = h
+
+    @classmethod
+    def for_problem(cls, prob, nx, ny, p, rknstg=3):
+        return cls(nx, ny, p, rknstg, prob.domain, prob.gamma, prob.bc_kind, prob.bc_state)
+
+    # -------------------------------------------------------------------------- life cycle
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def device_bytes(self):
+        b = C.c_size_t()
+        _check("mhd_gpu_device_bytes", self.lib.mhd_gpu_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def set_stream(self, stream_handle):
+        _check("mhd_gpu_set_stream", self.lib.mhd_gpu_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    def synchronize(self):
+        _check("mhd_gpu_synchronize", self.lib.mhd_gpu_synchronize(self.h))
+
+    # -------------------------------------------------------------------------- geometry
+    def nodes(self):
+        xx = np.zeros((self.p + 1, self.nx), order="F")
+        yy = np.zeros((self.p + 1, self.ny), order="F")
+        _check("mhd_gpu_nodes", self.lib.mhd_gpu_nodes(self.h, _p(xx), _p(yy)))
+        return xx, yy
+
+    def ldf_operator(self):
+        return ldf_operator(self.p, (self.domain[1] - self.domain[0]) / self.nx,
+                            (self.domain[3] - self.domain[2]) / self.ny)
+
+    # -------------------------------------------------------------------------- transfers
+    def upload_state(self, slot, u):
+        u = np.asfortranarray(u, dtype=np.float64)
+        assert u.shape == self.shape_u, (u.shape, self.shape_u)
+        _check("mhd_gpu_upload_state", self.lib.mhd_gpu_upload_state(self.h, slot, _p(u)))
+
+    def download_state(self, slot, out=None):
+        if out is None:
+            out = np.empty(self.shape_u, order="F")
+        _check("mhd_gpu_download_state", self.lib.mhd_gpu_download_state(self.h, slot, _p(out)))
+        return out
+
+    def upload_ut(self, stage, ut):
+        ut = np.asfortranarray(ut, dtype=np.float64)
+        assert ut.shape == self.shape_ut
+        _check("mhd_gpu_upload_ut", self.lib.mhd_gpu_upload_ut(self.h, stage, _p(ut)))
+
+    def download_ut(self, stage, out=None):
+        if out is None:
+            out = np.empty(self.shape_ut, order="F")
+        _check("mhd_gpu_download_ut", self.lib.mhd_gpu_download_ut(self.h, stage, _p(out)))
+        return out
+
+    def download_avg(self):
+        out = np.empty(self.shape_avg, order="F")
+        _check("mhd_gpu_download_avg", self.lib.mhd_gpu_download_avg(self.h, _p(out)))
+        return out
+
+    def state_device_ptr(self, slot):
+        p = _dp()
+        _check("mhd_gpu_state_device_ptr", self.lib.mhd_gpu_state_device_ptr(self.h, slot, C.byref(p)))
+        return C.cast(p, C.c_void_p).value
+
+    # -------------------------------------------------------------------------- reference calls
+    def apply_bc(self, slot):
+        _check("mhd_gpu_apply_bc", self.lib.mhd_gpu_apply_bc(self.h, slot))
+
+    def post_process(self, slot, apply_oedg, apply_ldf, oedg_dt, ent_offset, comput_ent):
+        neg, nneg = C.c_int(), C.c_int()
+        tot = C.c_double()
+        rc = self.lib.mhd_gpu_post_process(self.h, slot, int(apply_oedg), int(apply_ldf),
+                                           float(oedg_dt), int(ent_offset), int(comput_ent),
+                                           C.byref(neg), C.byref(nneg), C.byref(tot))
+        _check("mhd_gpu_post_process", rc, fatal_flags=False)
+        return dict(neg_avg=bool(neg.value), num_negcell=nneg.value, tot_ent=tot.value,
+                    pp_relimit_fail=bool(rc & capi.MHD_FLAG_PP_RELIMIT))
+
+    def semidiscretize(self, ut_stage, slot):
+        d = C.c_double()
+        _check("mhd_gpu_semidiscretize", self.lib.mhd_gpu_semidiscretize(self.h, ut_stage, slot, C.byref(d)))
+        return d.value
+
+    def rk_combine(self, stage, dt):
+        _check("mhd_gpu_rk_combine", self.lib.mhd_gpu_rk_combine(self.h, stage, float(dt)))
+
+    # -------------------------------------------------------------------------- driver
+    def solve_begin(self, final_T, cfl, use_oedg=True, use_ldf=True, ent_offset=False):
+        te, dl = C.c_double(), C.c_double()
+        rc = self.lib.mhd_gpu_solve_begin(self.h, float(final_T), float(cfl), int(use_oedg),
+                                          int(use_ldf), int(ent_offset), C.byref(te), C.byref(dl))
+        _check("mhd_gpu_solve_begin", rc)
+        return dict(tot_ent=te.value, dt_lim=dl.value)
+
+    def step(self):
+        st = Status()
+        rc = self.lib.mhd_gpu_step(self.h, C.byref(st))
+        _check("mhd_gpu_step", rc)
+        return st.as_dict()
+
+    def advance(self, max_steps=0, check_every=16, raise_on_flags=True):
+        st = Status()
+        rc = self.lib.mhd_gpu_advance(self.h, int(max_steps), int(check_every), C.byref(st))
+        _check("mhd_gpu_advance", rc, fatal_flags=raise_on_flags)
+        return st.as_dict()
+
+    def status(self):
+        st = Status()
+        rc = self.lib.mhd_gpu_get_status(self.h, C.byref(st))
+        _check("mhd_gpu_get_status", rc, fatal_flags=False)
+        return st.as_dict()
+
+    def solve_execute(self, u0, final_T, cfl, use_oedg=True, use_ldf=True, ent_offset=False,
+                      max_steps=0):
+        """solve_execute (drive.f90:32-343) from the initial state u0 (Fortran layout)."""
+        self.upload_state(0, u0)
+        info = self.solve_begin(final_T, cfl, use_oedg, use_ldf, ent_offset)
+        st = self.advance(max_steps)
+        st["initial"] = info
+        return st

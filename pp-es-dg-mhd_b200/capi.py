@@ -1,0 +1,97 @@
+"""ctypes binding of the C ABI in include/mhd_gpu.h (libmhd_gpu.so, built in-tree).
+
+There is no fallback: if the shared library is missing or cannot be loaded this module raises,
+and every solver call goes through the CUDA kernels.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmhd_gpu.so")
+
+MHD_OK = 0
+MHD_FLAG_NEG_AVG = 1
+MHD_FLAG_PP_RELIMIT = 2
+MHD_FLAG_DT_COLLAPSE = 4
+MHD_FLAG_INIT_NEG_AVG = 8
+MHD_ERR_INVALID = -1
+MHD_ERR_UNSUPPORTED = -2
+MHD_ERR_CUDA = -3
+MHD_ERR_NO_DEVICE = -4
+MHD_ERR_STATE = -5
+
+BC_PERIODIC, BC_EXTRAPOLATE, BC_FIXED, BC_XEXTRAP_YPER = 0, 1, 2, 3
+
+
+class Status(C.Structure):
+    """mhd_gpu_status"""
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("dt_lim", C.c_double),
+                ("tot_ent", C.c_double), ("steps", C.c_longlong), ("retries", C.c_longlong),
+                ("num_negcell_total", C.c_longlong), ("num_negcell_last", C.c_int),
+                ("done", C.c_int), ("flags", C.c_int), ("pad_", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+# name -> (restype, argtypes); exactly the functions declared in include/mhd_gpu.h
+SIGNATURES = {
+    "mhd_gpu_create": (C.c_int, [C.c_int] * 5 + [C.c_double] * 5 + [C.c_int, _dp, C.POINTER(_vp)]),
+    "mhd_gpu_destroy": (C.c_int, [_vp]),
+    "mhd_gpu_set_stream": (C.c_int, [_vp, _vp]),
+    "mhd_gpu_device_bytes": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "mhd_gpu_synchronize": (C.c_int, [_vp]),
+    "mhd_gpu_status_string": (C.c_char_p, [C.c_int]),
+    "mhd_gpu_nodes": (C.c_int, [_vp, _dp, _dp]),
+    "mhd_gpu_gll_tables": (C.c_int, [C.c_int] + [_dp] * 7),
+    "mhd_gpu_ldf_operator": (C.c_int, [C.c_int, C.c_double, C.c_double, _dp]),
+    "mhd_gpu_upload_state": (C.c_int, [_vp, C.c_int, _dp]),
+    "mhd_gpu_download_state": (C.c_int, [_vp, C.c_int, _dp]),
+    "mhd_gpu_upload_ut": (C.c_int, [_vp, C.c_int, _dp]),
+    "mhd_gpu_download_ut": (C.c_int, [_vp, C.c_int, _dp]),
+    "mhd_gpu_download_avg": (C.c_int, [_vp, _dp]),
+    "mhd_gpu_apply_bc": (C.c_int, [_vp, C.c_int]),
+    "mhd_gpu_post_process": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                       _ip, _ip, _dp]),
+    "mhd_gpu_semidiscretize": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
+    "mhd_gpu_rk_combine": (C.c_int, [_vp, C.c_int, C.c_double]),
+    "mhd_gpu_solve_begin": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp]),
+    "mhd_gpu_step": (C.c_int, [_vp, C.POINTER(Status)]),
+    "mhd_gpu_advance": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(Status)]),
+    "mhd_gpu_get_status": (C.c_int, [_vp, C.POINTER(Status)]),
+    "mhd_gpu_state_device_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_dp)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libmhd_gpu.so (raises if it is missing: there is no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libmhd_gpu.so not built ({path}); run pp-es-dg-mhd_b200/build.py")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)  # AttributeError if a declared symbol is not exported
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def status_string(code: int) -> str:
+    return load().mhd_gpu_status_string(int(code)).decode()
+
+
+class MHDError(RuntimeError):
+    """A C-ABI call returned an API error (< 0) or a fatal solver flag."""
+
+    def __init__(self, fn, code):
+        self.code = code
+        super().__init__(f"{fn} failed: {code} ({status_string(code)})")

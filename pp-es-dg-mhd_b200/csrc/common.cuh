@@ -1,0 +1,260 @@
+// common.cuh -- shared device definitions of the sm_100a DG-MHD stage pipeline.
+//
+// Device data layout (HBM): a state is element-blocked,
+//     u[ j ][ i ][ var ][ node ],  j in 0..ny+1, i in 0..nx+1 (one ghost ring),
+// node = k + n*l with n = p+1 GLL nodes per direction, var in 0..7 = (rho, mx, my, mz, Bx, By,
+// Bz, E).  One element block is 8*n*n doubles (256 B at p=1, 576 B at p=2, 1 KiB at p=3), so a
+// row of a tile of elements is one contiguous, 16-byte aligned run and every kernel moves tiles
+// with 128-bit loads.  The time derivative ut has the same per-element blocks without the ghost
+// ring: ut[ j-1 ][ i-1 ][ var ][ node ].
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mhd {
+
+constexpr double PP_EPS = 1.0e-11;   // DG_solver.f90:17
+constexpr double OEDG_EPS = 1.0e-8;  // DG_solver.f90:148
+constexpr int MAXP = 3;              // kernels are instantiated for p = 1, 2, 3
+constexpr int MAXN = MAXP + 1;
+
+// Per-degree tables in constant memory (gauss.f90 tables computed on the host).
+struct DegConst {
+  double qx[MAXN];          // GLL nodes
+  double qw[MAXN];          // GLL weights
+  double D[MAXN * MAXN];    // nodal differentiation matrix, column-major D[i + n*j]
+  double R0[MAXN][MAXN];    // R0[kk][k] = (D^kk)(0,k)    first row of D^kk
+  double RN[MAXN][MAXN];    // RN[kk][k] = (D^kk)(n-1,k)  last row of D^kk
+};
+// Defined here: the device code of the library is one translation unit (mhd_gpu.cu).
+__constant__ DegConst c_deg[MAXP + 1];
+
+// Gate values: a kernel launched with gate >= 0 runs only if ctrl->state == gate.
+enum GateState : int { GATE_ALWAYS = -1, ST_IDLE = 0, ST_RUN = 1, ST_RECOMPUTE = 2, ST_FAILED = 3 };
+
+// Device-resident control block: the scalars of solve_execute (drive.f90:39-48) and the global
+// reductions of post_process / DG_semidiscretize.
+struct Ctrl {
+  double t, dt, dt_lim, final_T, cfl_total, tot_ent;
+  double t_rk[6];
+  double u_avg_global[8];   // DG_solver.f90:146,228
+  double u_vari[8];         // DG_solver.f90:146,288
+  unsigned long long dt_lim_bits;  // atomicMin target, bit pattern of a positive double
+  unsigned long long umax_bits[8]; // order-preserving encodings for atomicMax/atomicMin
+  unsigned long long umin_bits[8];
+  long long steps, retries, num_negcell_total;
+  long long step_limit;  // ctl_step_begin idles once steps >= step_limit
+  int state;
+  int try_num;
+  int last_step;     // flag == .false. in drive.f90:115-120
+  int done;
+  int flags;         // MHD_FLAG_* bits
+  int neg_avg;       // post_process out (this stage)
+  int num_negcell;   // post_process out (this stage)
+  int num_negcell_last;
+  int pp_relimit;
+  int pending_dtlim; // a residual wrote dt_lim_bits that is not yet decoded
+  int pad_[2];
+};
+
+// Per-instance geometry passed by value.
+struct Geo {
+  int nx, ny;
+  double hx, hy, gamma;
+  int bc_kind;
+  int pad_;
+  double bc_state[8];
+  const double* ldfA;  // dense LDF nodal operator (2n^2 x 2n^2, column-major), device memory
+};
+
+// ---- order-preserving encodings of doubles for atomicMax / atomicMin --------------------------
+__device__ __forceinline__ unsigned long long ord_enc(double x) {
+  long long b = __double_as_longlong(x);
+  return b < 0 ? ~(unsigned long long)b : ((unsigned long long)b | 0x8000000000000000ULL);
+}
+__device__ __forceinline__ double ord_dec(unsigned long long e) {
+  return (e & 0x8000000000000000ULL) ? __longlong_as_double((long long)(e & 0x7FFFFFFFFFFFFFFFULL))
+                                     : __longlong_as_double((long long)~e);
+}
+
+__device__ __forceinline__ bool gate_open(const Ctrl* c, int gate) {
+  return gate < 0 || c->state == gate;
+}
+
+// ---- physics (MHD_PDE.f90 formulas as inlined in DG_solver.f90) -------------------------------
+
+// _macro_prs_ (DG_solver.f90:125)
+__device__ __forceinline__ double prs_of(double rho, double mx, double my, double mz, double bx,
+                                         double by, double bz, double e, double gamma) {
+  return (gamma - 1.0) * (e - 0.5 * ((mx * mx + my * my + mz * mz) / rho + (bx * bx + by * by + bz * bz)));
+}
+// _macro_ent_ (DG_solver.f90:126)
+__device__ __forceinline__ double ent_of(double rho, double prs, double gamma) {
+  return -(rho * (log(prs) - gamma * log(rho)) / (gamma - 1.0));
+}
+
+// log_avg_divisor (DG_solver.f90:1652-1681): 0.5*(a+b)/ff is the logarithmic mean of a and b.
+__device__ __forceinline__ double log_avg_divisor(double LL, double RR) {
+  const double zeta = LL / RR;
+  const double f = (zeta - 1.0) / (zeta + 1.0);
+  const double u = f * f;
+  if (u < 1.4e-4) return 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0)));
+  return 0.5 * log(zeta) / f;
+}
+
+// Entropy-conservative two-point flux, x (DIR=0, DG_solver.f90:1570-1609) or y (DIR=1,
+// DG_solver.f90:1611-1650).  a, b = (rho, vx, vy, vz, bx, by, bz, beta).
+template <int DIR>
+__device__ __forceinline__ void ec_flux(const double* a, const double* b, double gamma, double* f) {
+  const double rho_bar = 0.5 * (a[0] + b[0]);
+  const double vx_bar = 0.5 * (a[1] + b[1]);
+  const double vy_bar = 0.5 * (a[2] + b[2]);
+  const double vz_bar = 0.5 * (a[3] + b[3]);
+  const double bx_bar = 0.5 * (a[4] + b[4]);
+  const double by_bar = 0.5 * (a[5] + b[5]);
+  const double bz_bar = 0.5 * (a[6] + b[6]);
+  const double beta_bar = 0.5 * (a[7] + b[7]);
+  const double v_sq_bar = 0.5 * ((a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) + (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]));
+  const double b_sq_bar = 0.5 * ((a[4] * a[4] + a[5] * a[5] + a[6] * a[6]) + (b[4] * b[4] + b[5] * b[5] + b[6] * b[6]));
+  const double bvx = 0.5 * (a[7] * a[1] + b[7] * b[1]);
+  const double bvy = 0.5 * (a[7] * a[2] + b[7] * b[2]);
+  const double bvz = 0.5 * (a[7] * a[3] + b[7] * b[3]);
+  const double rho_hat = rho_bar / log_avg_divisor(a[0], b[0]);
+  const double beta_hat = beta_bar / log_avg_divisor(a[7], b[7]);
+  const double ptot = 0.5 * (b_sq_bar + rho_bar / beta_bar);
+  const double ecoef = 0.5 * (1.0 / ((gamma - 1.0) * beta_hat) - v_sq_bar);
+  const double vb = vx_bar * bx_bar + vy_bar * by_bar + vz_bar * bz_bar;
+  if (DIR == 0) {
+    f[0] = rho_hat * vx_bar;
+    f[1] = vx_bar * f[0] - bx_bar * bx_bar + ptot;
+    f[2] = vy_bar * f[0] - bx_bar * by_bar;
+    f[3] = vz_bar * f[0] - bx_bar * bz_bar;
+    f[4] = 0.0;
+    f[5] = (bvx * by_bar - bvy * bx_bar) / beta_bar;
+    f[6] = (bvx * bz_bar - bvz * bx_bar) / beta_bar;
+    f[7] = ecoef * f[0] + (vx_bar * f[1] + vy_bar * f[2] + vz_bar * f[3]) +
+           (bx_bar * f[4] + by_bar * f[5] + bz_bar * f[6]) - 0.5 * vx_bar * b_sq_bar + vb * bx_bar;
+  } else {
+    f[0] = rho_hat * vy_bar;
+    f[1] = vx_bar * f[0] - by_bar * bx_bar;
+    f[2] = vy_bar * f[0] - by_bar * by_bar + ptot;
+    f[3] = vz_bar * f[0] - by_bar * bz_bar;
+    f[4] = (bvy * bx_bar - bvx * by_bar) / beta_bar;
+    f[5] = 0.0;
+    f[6] = (bvy * bz_bar - bvz * by_bar) / beta_bar;
+    f[7] = ecoef * f[0] + (vx_bar * f[1] + vy_bar * f[2] + vz_bar * f[3]) +
+           (bx_bar * f[4] + by_bar * f[5] + bz_bar * f[6]) - 0.5 * vy_bar * b_sq_bar + vb * by_bar;
+  }
+}
+
+// ESPP_HLL_flux_x (DG_solver.f90:894-1071).  wl, wr: conserved states already rotated into the
+// face normal frame (swap_xy for y faces).  out[0..7] = numerical flux, out[8] = nBn,
+// out[9] = sl, out[10] = sr.
+__device__ __forceinline__ void espp_hll(const double* wl, const double* wr, double gamma, double* out) {
+  const double rho_l = wl[0], mx_l = wl[1], my_l = wl[2], mz_l = wl[3], bx_l = wl[4], by_l = wl[5], bz_l = wl[6], e_l = wl[7];
+  const double rho_r = wr[0], mx_r = wr[1], my_r = wr[2], mz_r = wr[3], bx_r = wr[4], by_r = wr[5], bz_r = wr[6], e_r = wr[7];
+  const double gm1 = gamma - 1.0;
+  const double ir_l = 1.0 / rho_l, ir_r = 1.0 / rho_r;
+  const double vx_l = ir_l * mx_l, vx_r = ir_r * mx_r;
+  const double vy_l = ir_l * my_l, vy_r = ir_r * my_r;
+  const double vz_l = ir_l * mz_l, vz_r = ir_r * mz_r;
+  const double ek_l = 0.5 * ir_l * (mx_l * mx_l + my_l * my_l + mz_l * mz_l);
+  const double ek_r = 0.5 * ir_r * (mx_r * mx_r + my_r * my_r + mz_r * mz_r);
+  const double bsq_l = bx_l * bx_l + by_l * by_l + bz_l * bz_l;
+  const double bsq_r = bx_r * bx_r + by_r * by_r + bz_r * bz_r;
+  const double pm_l = 0.5 * bsq_l, pm_r = 0.5 * bsq_r;
+  const double p_l = fmax(gm1 * (e_l - (ek_l + pm_l)), PP_EPS);
+  const double p_r = fmax(gm1 * (e_r - (ek_r + pm_r)), PP_EPS);
+  const double pt_l = p_l + pm_l, pt_r = p_r + pm_r;
+  const double bu_l = bx_l * vx_l + by_l * vy_l + bz_l * vz_l;
+  const double bu_r = bx_r * vx_r + by_r * vy_r + bz_r * vz_r;
+  const double cs_l = gamma * p_l * ir_l, cs_r = gamma * p_r * ir_r;
+  const double ss_l = cs_l + bsq_l * ir_l, ss_r = cs_r + bsq_r * ir_r;
+  const double cf_l = sqrt(0.5 * (ss_l + sqrt(fmax(ss_l * ss_l - 4.0 * cs_l * ir_l * (bx_l * bx_l), 0.0))));
+  const double cf_r = sqrt(0.5 * (ss_r + sqrt(fmax(ss_r * ss_r - 4.0 * cs_r * ir_r * (bx_r * bx_r), 0.0))));
+  const double ith_l = rho_l / p_l, ith_r = rho_r / p_r;
+  const double phi_l = ith_l * bu_l, phi_r = ith_r * bu_r;
+  const double se_l = log(p_l) - gamma * log(rho_l);
+  const double se_r = log(p_r) - gamma * log(rho_r);
+  const double ef_l = (-rho_l * se_l / gm1) * vx_l;
+  const double ef_r = (-rho_r * se_r / gm1) * vx_r;
+  double fl[8], fr[8], vl[8], vr[8];
+  fl[0] = mx_l;
+  fl[1] = vx_l * mx_l - bx_l * bx_l + pt_l;
+  fl[2] = vx_l * my_l - by_l * bx_l;
+  fl[3] = vx_l * mz_l - bz_l * bx_l;
+  fl[4] = 0.0;
+  fl[5] = -(bx_l * vy_l - by_l * vx_l);
+  fl[6] = bz_l * vx_l - bx_l * vz_l;
+  fl[7] = vx_l * (e_l + pt_l) - bx_l * bu_l;
+  fr[0] = mx_r;
+  fr[1] = vx_r * mx_r - bx_r * bx_r + pt_r;
+  fr[2] = vx_r * my_r - by_r * bx_r;
+  fr[3] = vx_r * mz_r - bz_r * bx_r;
+  fr[4] = 0.0;
+  fr[5] = -(bx_r * vy_r - by_r * vx_r);
+  fr[6] = bz_r * vx_r - bx_r * vz_r;
+  fr[7] = vx_r * (e_r + pt_r) - bx_r * bu_r;
+  vl[0] = (gamma - se_l) / gm1 - ek_l / p_l;
+  vl[1] = mx_l / p_l;
+  vl[2] = my_l / p_l;
+  vl[3] = mz_l / p_l;
+  vl[4] = ith_l * bx_l;
+  vl[5] = ith_l * by_l;
+  vl[6] = ith_l * bz_l;
+  vl[7] = -ith_l;
+  vr[0] = (gamma - se_r) / gm1 - ek_r / p_r;
+  vr[1] = mx_r / p_r;
+  vr[2] = my_r / p_r;
+  vr[3] = mz_r / p_r;
+  vr[4] = ith_r * bx_r;
+  vr[5] = ith_r * by_r;
+  vr[6] = ith_r * bz_r;
+  vr[7] = -ith_r;
+  const double sq_l = sqrt(rho_l), sq_r = sqrt(rho_r);
+  const double sum_sq = sq_l + sq_r;
+  const double vx_roe = (vx_l * sq_l + vx_r * sq_r) / sum_sq;
+  const double db = sqrt((bx_l - bx_r) * (bx_l - bx_r) + (by_l - by_r) * (by_l - by_r) + (bz_l - bz_r) * (bz_l - bz_r)) / sum_sq;
+  const double sl_pp = fmin(vx_l, vx_roe) - cf_l - db;
+  const double sr_pp = fmax(vx_r, vx_roe) + cf_r + db;
+  double da = 0.0, dbl = 0.0, dbr = 0.0;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const double dfs = fr[s] - fl[s];
+    da += (vr[s] - vl[s]) * (wr[s] - wl[s]);
+    dbl += vl[s] * dfs;
+    dbr += vr[s] * dfs;
+  }
+  const double a_form = fmax(da, 0.0) + 1e-8;
+  const double bl_form = (ef_r - ef_l) - dbl - phi_l * (bx_r - bx_l);
+  const double br_form = (ef_r - ef_l) - dbr - phi_r * (bx_r - bx_l);
+  const double al = fmax(bl_form / a_form, 0.0);
+  const double ar = fmax(br_form / a_form, 0.0);
+  const double aa = sqrt(al * ar);
+  const double sl = fmin(fmin(-(ar + aa), sl_pp), 0.0);
+  const double sr = fmax(fmax(al + aa, sr_pp), 0.0);
+  const double dslr = sr - sl;
+  const double wl_ = sr / dslr, wr_ = -sl / dslr, wd = (sl * sr) / dslr;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) out[s] = wl_ * fl[s] + wr_ * fr[s] + wd * (wr[s] - wl[s]);
+  out[8] = wl_ * bx_l + wr_ * bx_r;
+  out[9] = sl;
+  out[10] = sr;
+}
+
+// max fast magnetosonic speed of a node in x and y (DG_solver.f90:749-770)
+__device__ __forceinline__ void node_sigma(const double* w, double gamma, double& sx, double& sy) {
+  const double rho = w[0];
+  const double ir = 1.0 / rho;
+  const double vx = ir * w[1], vy = ir * w[2];
+  const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+  const double bsq = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
+  const double pf = fmax((gamma - 1.0) * (w[7] - (ek + 0.5 * bsq)), PP_EPS);
+  const double cs = gamma * pf * ir;
+  const double ss = cs + bsq * ir;
+  const double coef = 4.0 * cs * ir;
+  sx = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
+  sy = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
+}
+
+}  // namespace mhd

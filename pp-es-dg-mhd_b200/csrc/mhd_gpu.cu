@@ -1,0 +1,614 @@
+// mhd_gpu.cu -- C ABI (include/mhd_gpu.h) of the sm_100a DG-MHD stage pipeline.
+//
+// The handle replaces the reference's module-level state (DG_solver.f90:6-43) with device
+// allocations; every entry point maps onto one reference procedure (see mhd_gpu.h).  The
+// device-resident driver replays solve_execute's try/stage sequence (drive.f90:83-320) as one
+// captured CUDA graph per time-step try: control decisions (dt, retry, acceptance) are made by
+// single-thread control kernels on the device, so the host only polls a status block.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "../../include/mhd_gpu.h"
+#include "common.cuh"
+#include "misc.cuh"
+#include "post.cuh"
+#include "residual.cuh"
+#include "tables.h"
+
+using namespace mhd;
+
+struct mhd_gpu {
+  int nx, ny, p, n, nn, eb, R, bc_kind;
+  double left, right, bottom, top, hx, hy, gamma, bc_state[8];
+  int device;
+  cudaStream_t stream;
+  cudaStream_t own_stream;
+  double* u[6];   // slot 0 = u_con, s = uRK_con(:,s)
+  double* ut[6];  // 1..R
+  double* u_avg;
+  double* staging;
+  double* ldfA;
+  double* sig_x;
+  double* sig_y;
+  double* partial;
+  double* ent_partial;
+  double* cell_ent_DG;
+  double* cell_ent_FV;
+  unsigned char* cell_ent_nan;
+  Ctrl* ctrl;
+  Ctrl* ctrl_host;  // pinned mirror
+  size_t bytes;
+  Geo geo;
+  // device-resident driver
+  int solve_ready;
+  double final_T, cfl;
+  int use_oedg, use_ldf, ent_offset;
+  cudaGraphExec_t step_exec;
+};
+
+namespace {
+
+const int kMaxDevices = 64;
+std::mutex g_init_mutex;
+bool g_dev_init[kMaxDevices];
+
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return MHD_ERR_CUDA;   \
+  } while (0)
+
+long long n_state(const mhd_gpu* h) { return (long long)(h->nx + 2) * (h->ny + 2) * h->eb; }
+long long n_ut(const mhd_gpu* h) { return (long long)h->nx * h->ny * h->eb; }
+int grid1d(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+template <int P>
+int pp_nblk_avg(const mhd_gpu* h) { return grid1d((long long)(h->nx + 2) * (h->ny + 2), PPCfg<P>::TE); }
+template <int P>
+dim3 pp_grid_limit(const mhd_gpu* h) { return dim3((h->nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE, h->ny); }
+
+int init_device_tables(int dev) {
+  std::lock_guard<std::mutex> lk(g_init_mutex);
+  if (dev < 0 || dev >= kMaxDevices) return MHD_ERR_INVALID;
+  if (g_dev_init[dev]) return MHD_OK;
+  DegConst tabs[MAXP + 1];
+  std::memset(tabs, 0, sizeof(tabs));
+  for (int p = 1; p <= MAXP; ++p) {
+    const int n = p + 1;
+    double x[8], w[8], D[64], R0[64], RN[64];
+    if (tables::gll(p, x, w, nullptr, nullptr, D, nullptr, nullptr)) return MHD_ERR_INVALID;
+    if (tables::dpow_rows(p, R0, RN)) return MHD_ERR_INVALID;
+    for (int i = 0; i < n; ++i) {
+      tabs[p].qx[i] = x[i];
+      tabs[p].qw[i] = w[i];
+    }
+    for (int i = 0; i < n * n; ++i) tabs[p].D[i] = D[i];
+    for (int kk = 0; kk <= p; ++kk)
+      for (int k = 0; k < n; ++k) {
+        tabs[p].R0[kk][k] = R0[kk * n + k];
+        tabs[p].RN[kk][k] = RN[kk * n + k];
+      }
+  }
+  CK(cudaMemcpyToSymbol(c_deg, tabs, sizeof(tabs)));
+  CK(cudaFuncSetAttribute(residual_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
+  g_dev_init[dev] = true;
+  return MHD_OK;
+}
+
+int enter(const mhd_gpu* h) {
+  if (!h) return MHD_ERR_INVALID;
+  CK(cudaSetDevice(h->device));
+  return MHD_OK;
+}
+
+// ---- launchers ---------------------------------------------------------------------------
+template <int P>
+void launch_bc(mhd_gpu* h, double* u, int gate) {
+  constexpr int EB = 8 * (P + 1) * (P + 1);
+  const long long n = 2LL * (h->nx + h->ny) * EB;
+  bc_kernel<P><<<grid1d(n, 256), 256, 0, h->stream>>>(u, h->geo, h->ctrl, gate);
+}
+
+template <int P>
+void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate) {
+  using L = ResLayout<P>;
+  dim3 grid((h->nx + L::TX - 1) / L::TX, (h->ny + L::TY - 1) / L::TY);
+  residual_kernel<P><<<grid, ResCfg<P>::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate);
+}
+
+template <int P>
+void launch_combine(mhd_gpu* h, int stage, const double* dt_ptr, double dt, int gate) {
+  constexpr int EB = 8 * (P + 1) * (P + 1);
+  const long long n = (long long)h->nx * h->ny * EB;
+  combine_kernel<EB><<<grid1d(n, 256), 256, 0, h->stream>>>(
+      h->u[0], h->u[1], h->R >= 2 ? h->u[2] : nullptr, h->R >= 3 ? h->u[3] : nullptr, h->R >= 4 ? h->u[4] : nullptr,
+      h->ut[1], h->R >= 2 ? h->ut[2] : nullptr, h->R >= 3 ? h->ut[3] : nullptr, h->R >= 4 ? h->ut[4] : nullptr,
+      h->R >= 5 ? h->ut[5] : nullptr, h->u[stage], h->nx, h->ny, h->R, stage, dt_ptr, dt, h->ctrl, gate);
+}
+
+// post_process on slot `slot` (everything but the control-block reset and the host read-back)
+template <int P>
+void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const double* dt_ptr, double oedg_dt,
+                 int ent_offset, int comput_ent, double* accept_dst, int gate) {
+  const int nb1 = pp_nblk_avg<P>(h);
+  pp_avg_ldf_kernel<P><<<nb1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
+                                                      apply_oedg, ent_offset, h->partial, h->cell_ent_DG,
+                                                      h->cell_ent_FV, h->cell_ent_nan);
+  if (apply_oedg) {
+    pp_reduce_kernel<<<1, 256, 0, h->stream>>>(h->partial, nb1, h->ctrl, gate);
+    const long long nf = ((long long)(h->nx + 1) * h->ny + (long long)h->nx * (h->ny + 1)) * 8;
+    pp_sigsum_kernel<P><<<grid1d(nf, 256), 256, 0, h->stream>>>(h->u[slot], h->geo, h->ctrl, gate, h->sig_x, h->sig_y);
+  }
+  dim3 g3 = pp_grid_limit<P>(h);
+  pp_limit_kernel<P><<<g3, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_oedg, dt_ptr,
+                                                   oedg_dt, ent_offset, comput_ent, h->sig_x, h->sig_y,
+                                                   h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan,
+                                                   h->ent_partial, accept_dst);
+  if (comput_ent) pp_entsum_kernel<<<1, 256, 0, h->stream>>>(h->ent_partial, (int)(g3.x * g3.y), h->ctrl, gate);
+}
+
+#define DISPATCH_P(h, fn, ...)              \
+  do {                                      \
+    switch ((h)->p) {                       \
+      case 1: fn<1>(__VA_ARGS__); break;    \
+      case 2: fn<2>(__VA_ARGS__); break;    \
+      default: fn<3>(__VA_ARGS__); break;   \
+    }                                       \
+  } while (0)
+
+int read_ctrl(mhd_gpu* h) {
+  CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+
+void fill_status(const mhd_gpu* h, mhd_gpu_status* st) {
+  if (!st) return;
+  const Ctrl* c = h->ctrl_host;
+  st->t = c->t;
+  st->dt = c->dt;
+  st->dt_lim = c->dt_lim;
+  st->tot_ent = c->tot_ent;
+  st->steps = c->steps;
+  st->retries = c->retries;
+  st->num_negcell_total = c->num_negcell_total;
+  st->num_negcell_last = c->num_negcell_last;
+  st->done = c->done;
+  st->flags = c->flags;
+  st->pad_ = 0;
+}
+
+// one try of a time step (drive.f90:93-300), recorded into the capturing stream
+template <int P>
+void enqueue_try(mhd_gpu* h) {
+  const int R = h->R;
+  ctl_step_begin<<<1, 1, 0, h->stream>>>(h->ctrl);
+  launch_residual<P>(h, h->u[0], h->ut[1], ST_RECOMPUTE);
+  ctl_dt<<<1, 1, 0, h->stream>>>(h->ctrl);
+  for (int s = 1; s <= R; ++s) {
+    const int fin = (s == R);
+    ctl_stage_time<<<1, 1, 0, h->stream>>>(h->ctrl, R, s);
+    launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
+    launch_bc<P>(h, h->u[s], ST_RUN);
+    launch_post<P>(h, s, h->use_oedg && fin, h->use_ldf, &h->ctrl->dt, 0.0, h->ent_offset, fin,
+                   fin ? h->u[0] : nullptr, ST_RUN);
+    ctl_stage_end<<<1, 1, 0, h->stream>>>(h->ctrl);
+    launch_bc<P>(h, h->u[s], ST_RUN);
+    launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN);
+  }
+  ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R);
+}
+
+int build_step_graph(mhd_gpu* h) {
+  if (h->step_exec) {
+    cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+  }
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  DISPATCH_P(h, enqueue_try, h);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+  if (e != cudaSuccess) return MHD_ERR_CUDA;
+  e = cudaGraphInstantiate(&h->step_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return MHD_ERR_CUDA;
+  return MHD_OK;
+}
+
+void free_all(mhd_gpu* h) {
+  if (!h) return;
+  if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  for (int s = 0; s < 6; ++s) {
+    if (h->u[s]) cudaFree(h->u[s]);
+    if (h->ut[s]) cudaFree(h->ut[s]);
+  }
+  void* ptrs[] = {h->u_avg, h->staging, h->ldfA, h->sig_x, h->sig_y, h->partial, h->ent_partial,
+                  h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan, h->ctrl};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+}
+
+}  // namespace
+
+// =============================================================================================
+extern "C" {
+
+const char* mhd_gpu_status_string(int code) {
+  switch (code) {
+    case MHD_OK: return "ok";
+    case MHD_FLAG_NEG_AVG: return "inadmissible cell average";
+    case MHD_FLAG_PP_RELIMIT: return "positivity re-limit failed";
+    case MHD_FLAG_DT_COLLAPSE: return "time step collapsed (too many re-tries or dt_lim < 1e-14)";
+    case MHD_FLAG_INIT_NEG_AVG: return "initial value has an inadmissible cell average";
+    case MHD_ERR_INVALID: return "invalid argument";
+    case MHD_ERR_UNSUPPORTED: return "unsupported configuration";
+    case MHD_ERR_CUDA: return "CUDA runtime error";
+    case MHD_ERR_NO_DEVICE: return "no CUDA device";
+    case MHD_ERR_STATE: return "call out of order";
+    default: return "solver flags set";
+  }
+}
+
+int mhd_gpu_gll_tables(int p, double* x, double* w, double* M, double* Minv, double* D, double* Pmn, double* Pnm) {
+  if (p < 0 || p > 6) return MHD_ERR_INVALID;
+  return tables::gll(p, x, w, M, Minv, D, Pmn, Pnm) ? MHD_ERR_INVALID : MHD_OK;
+}
+
+int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, double right, double bottom,
+                   double top, double gamma, int bc_kind, const double* bc_state8, mhd_gpu_t** out) {
+  if (!out) return MHD_ERR_INVALID;
+  *out = nullptr;
+  if (nx < 2 || ny < 2 || !(right > left) || !(top > bottom) || !(gamma > 1.0)) return MHD_ERR_INVALID;
+  if (px != py || px < 1 || px > MAXP) return MHD_ERR_UNSUPPORTED;
+  if (!(rknstg == 1 || rknstg == 2 || rknstg == 3 || rknstg == 5)) return MHD_ERR_UNSUPPORTED;
+  if (bc_kind < 0 || bc_kind > 3) return MHD_ERR_INVALID;
+  if (bc_kind == MHD_BC_FIXED && !bc_state8) return MHD_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MHD_ERR_NO_DEVICE;
+  mhd_gpu* h = new (std::nothrow) mhd_gpu;
+  if (!h) return MHD_ERR_INVALID;
+  std::memset(h, 0, sizeof(*h));
+  if (cudaGetDevice(&h->device) != cudaSuccess) {
+    delete h;
+    return MHD_ERR_CUDA;
+  }
+  int rc = init_device_tables(h->device);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  h->nx = nx;
+  h->ny = ny;
+  h->p = px;
+  h->n = px + 1;
+  h->nn = h->n * h->n;
+  h->eb = 8 * h->nn;
+  h->R = rknstg;
+  h->bc_kind = bc_kind;
+  h->left = left;
+  h->right = right;
+  h->bottom = bottom;
+  h->top = top;
+  h->gamma = gamma;
+  h->hx = (right - left) / nx;  // DG_solver.f90:93-94
+  h->hy = (top - bottom) / ny;
+  for (int v = 0; v < 8; ++v) h->bc_state[v] = bc_state8 ? bc_state8[v] : 0.0;
+#define ALLOC(ptr, bytes_)                                               \
+  do {                                                                   \
+    size_t b_ = (size_t)(bytes_);                                        \
+    if (cudaMalloc((void**)&(ptr), b_ ? b_ : 16) != cudaSuccess) {       \
+      free_all(h);                                                       \
+      delete h;                                                          \
+      return MHD_ERR_CUDA;                                               \
+    }                                                                    \
+    h->bytes += b_;                                                      \
+  } while (0)
+  const size_t sb = sizeof(double) * (size_t)n_state(h), tb = sizeof(double) * (size_t)n_ut(h);
+  for (int s = 0; s <= rknstg; ++s) ALLOC(h->u[s], sb);
+  for (int s = 1; s <= rknstg; ++s) ALLOC(h->ut[s], tb);
+  const long long nelg = (long long)(nx + 2) * (ny + 2);
+  ALLOC(h->u_avg, sizeof(double) * 8 * nelg);
+  ALLOC(h->staging, sb);
+  const int n2 = 2 * h->nn;
+  ALLOC(h->ldfA, sizeof(double) * n2 * n2);
+  ALLOC(h->sig_x, sizeof(double) * 8 * (size_t)(nx + 1) * ny);
+  ALLOC(h->sig_y, sizeof(double) * 8 * (size_t)nx * (ny + 1));
+  const int te_min = 16;
+  ALLOC(h->partial, sizeof(double) * 8 * (size_t)((nelg + te_min - 1) / te_min + 1));
+  ALLOC(h->ent_partial, sizeof(double) * (size_t)((nx + te_min - 1) / te_min + 1) * ny);
+  ALLOC(h->cell_ent_DG, sizeof(double) * nelg);
+  ALLOC(h->cell_ent_FV, sizeof(double) * nelg);
+  ALLOC(h->cell_ent_nan, nelg);
+  ALLOC(h->ctrl, sizeof(Ctrl));
+#undef ALLOC
+  if (cudaMallocHost((void**)&h->ctrl_host, sizeof(Ctrl)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    free_all(h);
+    delete h;
+    return MHD_ERR_CUDA;
+  }
+  h->stream = h->own_stream;
+  // NaN-filled state, as the reference allocates with ieee_signaling_nan (DG_solver.f90:56,68-71)
+  for (int s = 0; s <= rknstg; ++s) cudaMemsetAsync(h->u[s], 0xFF, sb, h->stream);
+  for (int s = 1; s <= rknstg; ++s) cudaMemsetAsync(h->ut[s], 0xFF, tb, h->stream);
+  cudaMemsetAsync(h->u_avg, 0xFF, sizeof(double) * 8 * nelg, h->stream);
+  cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), h->stream);
+  double A[32 * 32];
+  tables::ldf_nodal_operator(px, h->hx, h->hy, A);
+  cudaMemcpyAsync(h->ldfA, A, sizeof(double) * n2 * n2, cudaMemcpyHostToDevice, h->stream);
+  h->geo.nx = nx;
+  h->geo.ny = ny;
+  h->geo.hx = h->hx;
+  h->geo.hy = h->hy;
+  h->geo.gamma = gamma;
+  h->geo.bc_kind = bc_kind;
+  for (int v = 0; v < 8; ++v) h->geo.bc_state[v] = h->bc_state[v];
+  h->geo.ldfA = h->ldfA;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    free_all(h);
+    delete h;
+    return MHD_ERR_CUDA;
+  }
+  *out = h;
+  return MHD_OK;
+}
+
+int mhd_gpu_destroy(mhd_gpu_t* h) {
+  if (!h) return MHD_ERR_INVALID;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return MHD_OK;
+}
+
+int mhd_gpu_set_stream(mhd_gpu_t* h, void* stream) {
+  int rc = enter(h);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  h->solve_ready = 0;  // the step graph is recaptured on the new stream
+  return MHD_OK;
+}
+
+int mhd_gpu_device_bytes(const mhd_gpu_t* h, size_t* bytes) {
+  if (!h || !bytes) return MHD_ERR_INVALID;
+  *bytes = h->bytes;
+  return MHD_OK;
+}
+
+int mhd_gpu_synchronize(mhd_gpu_t* h) {
+  int rc = enter(h);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+
+int mhd_gpu_nodes(const mhd_gpu_t* h, double* xx, double* yy) {
+  if (!h) return MHD_ERR_INVALID;
+  double x[8], w[8];
+  tables::gll(h->p, x, w, nullptr, nullptr, nullptr, nullptr, nullptr);
+  const int n = h->n;
+  if (xx)  // DG_solver.f90:101-103
+    for (int i = 1; i <= h->nx; ++i)
+      for (int k = 0; k < n; ++k) xx[k + n * (i - 1)] = (0.5 * h->hx) * x[k] + (h->left + (i - 0.5) * h->hx);
+  if (yy)
+    for (int j = 1; j <= h->ny; ++j)
+      for (int l = 0; l < n; ++l) yy[l + n * (j - 1)] = (0.5 * h->hy) * x[l] + (h->bottom + (j - 0.5) * h->hy);
+  return MHD_OK;
+}
+
+int mhd_gpu_ldf_operator(int p, double hx, double hy, double* A) {
+  if (!A || p < 1 || p > 6 || !(hx > 0.0) || !(hy > 0.0)) return MHD_ERR_INVALID;
+  return tables::ldf_nodal_operator(p, hx, hy, A) ? MHD_ERR_INVALID : MHD_OK;
+}
+
+static int transfer_in(mhd_gpu* h, const double* src, double* dst, long long nelem) {
+  const long long n = nelem * h->eb;
+  CK(cudaMemcpyAsync(h->staging, src, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+  to_blocked_kernel<<<grid1d(n, 256), 256, 0, h->stream>>>(h->staging, dst, nelem, h->nn);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+static int transfer_out(mhd_gpu* h, const double* src, double* dst, long long nelem) {
+  const long long n = nelem * h->eb;
+  to_fortran_kernel<<<grid1d(n, 256), 256, 0, h->stream>>>(src, h->staging, nelem, h->nn);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dst, h->staging, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+
+int mhd_gpu_upload_state(mhd_gpu_t* h, int slot, const double* u) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!u || slot < 0 || slot > h->R) return MHD_ERR_INVALID;
+  return transfer_in(h, u, h->u[slot], (long long)(h->nx + 2) * (h->ny + 2));
+}
+int mhd_gpu_download_state(mhd_gpu_t* h, int slot, double* u) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!u || slot < 0 || slot > h->R) return MHD_ERR_INVALID;
+  return transfer_out(h, h->u[slot], u, (long long)(h->nx + 2) * (h->ny + 2));
+}
+int mhd_gpu_upload_ut(mhd_gpu_t* h, int stage, const double* ut) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!ut || stage < 1 || stage > h->R) return MHD_ERR_INVALID;
+  return transfer_in(h, ut, h->ut[stage], (long long)h->nx * h->ny);
+}
+int mhd_gpu_download_ut(mhd_gpu_t* h, int stage, double* ut) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!ut || stage < 1 || stage > h->R) return MHD_ERR_INVALID;
+  return transfer_out(h, h->ut[stage], ut, (long long)h->nx * h->ny);
+}
+int mhd_gpu_download_avg(mhd_gpu_t* h, double* u_avg) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!u_avg) return MHD_ERR_INVALID;
+  CK(cudaMemcpyAsync(u_avg, h->u_avg, sizeof(double) * 8 * (size_t)(h->nx + 2) * (h->ny + 2),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+
+int mhd_gpu_apply_bc(mhd_gpu_t* h, int slot) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (slot < 0 || slot > h->R) return MHD_ERR_INVALID;
+  DISPATCH_P(h, launch_bc, h, h->u[slot], GATE_ALWAYS);
+  CK(cudaGetLastError());
+  return MHD_OK;
+}
+
+int mhd_gpu_post_process(mhd_gpu_t* h, int slot, int apply_oedg, int apply_ldf, double oedg_dt, int ent_offset,
+                         int comput_ent, int* neg_avg, int* num_negcell, double* tot_ent) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (slot < 0 || slot > h->R) return MHD_ERR_INVALID;
+  ctl_pp_reset<<<1, 1, 0, h->stream>>>(h->ctrl, GATE_ALWAYS);
+  DISPATCH_P(h, launch_post, h, slot, apply_oedg != 0, apply_ldf != 0, nullptr, oedg_dt, ent_offset != 0,
+             comput_ent != 0, nullptr, GATE_ALWAYS);
+  CK(cudaGetLastError());
+  rc = read_ctrl(h);
+  if (rc) return rc;
+  const Ctrl* c = h->ctrl_host;
+  if (neg_avg) *neg_avg = c->neg_avg;
+  if (num_negcell) *num_negcell = c->neg_avg ? 0 : c->num_negcell;
+  if (tot_ent) *tot_ent = (c->neg_avg || !comput_ent) ? NAN : c->tot_ent;  // DG_solver.f90:660
+  return c->pp_relimit ? MHD_FLAG_PP_RELIMIT : MHD_OK;
+}
+
+int mhd_gpu_semidiscretize(mhd_gpu_t* h, int ut_stage, int slot, double* dt_lim) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (slot < 0 || slot > h->R || ut_stage < 1 || ut_stage > h->R) return MHD_ERR_INVALID;
+  CK(cudaMemsetAsync(&h->ctrl->dt_lim_bits, 0xFF, sizeof(unsigned long long), h->stream));
+  DISPATCH_P(h, launch_residual, h, h->u[slot], h->ut[ut_stage], GATE_ALWAYS);
+  CK(cudaGetLastError());
+  if (dt_lim) {
+    unsigned long long bits;
+    CK(cudaMemcpyAsync(&bits, &h->ctrl->dt_lim_bits, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double d;
+    std::memcpy(&d, &bits, sizeof(d));
+    *dt_lim = d;
+  }
+  return MHD_OK;
+}
+
+int mhd_gpu_rk_combine(mhd_gpu_t* h, int stage, double dt) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (stage < 1 || stage > h->R) return MHD_ERR_INVALID;
+  DISPATCH_P(h, launch_combine, h, stage, nullptr, dt, GATE_ALWAYS);
+  CK(cudaGetLastError());
+  return MHD_OK;
+}
+
+int mhd_gpu_solve_begin(mhd_gpu_t* h, double final_T, double cfl, int use_oedg, int use_ldf, int ent_offset,
+                        double* tot_ent, double* dt_lim) {
+  int rc = enter(h);
+  if (rc) return rc;
+  h->solve_ready = 0;
+  // drive.f90:67-73
+  rc = mhd_gpu_apply_bc(h, 0);
+  if (rc) return rc;
+  int neg = 0, nneg = 0;
+  double te = 0.0;
+  rc = mhd_gpu_post_process(h, 0, 0, use_ldf, 0.0, 0, 1, &neg, &nneg, &te);
+  if (rc < 0) return rc;
+  if (neg) return MHD_FLAG_INIT_NEG_AVG;
+  rc = mhd_gpu_apply_bc(h, 0);
+  if (rc) return rc;
+  double dl = 0.0;
+  rc = mhd_gpu_semidiscretize(h, 1, 0, &dl);
+  if (rc) return rc;
+  if (tot_ent) *tot_ent = te;
+  if (dt_lim) *dt_lim = dl;
+  h->final_T = final_T;
+  h->cfl = cfl;
+  h->use_oedg = use_oedg != 0;
+  h->use_ldf = use_ldf != 0;
+  h->ent_offset = ent_offset != 0;
+  Ctrl c;
+  std::memset(&c, 0, sizeof(c));
+  c.t = 0.0;
+  c.dt_lim = dl;
+  c.final_T = final_T;
+  c.cfl_total = ((h->R <= 3) ? 1.0 : 1.508) * cfl;  // CFL_RK * CFL (drive.f90:57-63,109)
+  c.tot_ent = te;
+  c.state = ST_IDLE;
+  c.step_limit = 0x7fffffffffffffffLL;
+  *h->ctrl_host = c;
+  CK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  rc = build_step_graph(h);
+  if (rc) return rc;
+  h->solve_ready = 1;
+  return MHD_OK;
+}
+
+static int set_step_limit(mhd_gpu* h, long long limit) {
+  CK(cudaMemcpyAsync(&h->ctrl->step_limit, &limit, sizeof(limit), cudaMemcpyHostToDevice, h->stream));
+  return MHD_OK;
+}
+
+int mhd_gpu_get_status(mhd_gpu_t* h, mhd_gpu_status* st) {
+  int rc = enter(h);
+  if (rc) return rc;
+  rc = read_ctrl(h);
+  if (rc) return rc;
+  fill_status(h, st);
+  return h->ctrl_host->flags;
+}
+
+int mhd_gpu_advance(mhd_gpu_t* h, long long max_steps, int check_every, mhd_gpu_status* st) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!h->solve_ready) return MHD_ERR_STATE;
+  if (check_every <= 0) check_every = 16;
+  rc = read_ctrl(h);
+  if (rc) return rc;
+  const long long start = h->ctrl_host->steps;
+  const long long target = (max_steps > 0) ? start + max_steps : 0x7fffffffffffffffLL;
+  rc = set_step_limit(h, target);
+  if (rc) return rc;
+  for (;;) {
+    const Ctrl* c = h->ctrl_host;
+    if (c->done || c->flags || c->steps >= target) break;
+    // tries left before the target: retries need extra launches, so never queue more than
+    // the remaining steps plus a small slack; extra launches past the target are idle.
+    long long left = target - c->steps;
+    int batch = (int)((left < check_every) ? left : check_every);
+    if (batch < 1) batch = 1;
+    for (int b = 0; b < batch; ++b) CK(cudaGraphLaunch(h->step_exec, h->stream));
+    rc = read_ctrl(h);
+    if (rc) return rc;
+  }
+  fill_status(h, st);
+  set_step_limit(h, 0x7fffffffffffffffLL);
+  CK(cudaStreamSynchronize(h->stream));
+  return h->ctrl_host->flags;
+}
+
+int mhd_gpu_step(mhd_gpu_t* h, mhd_gpu_status* st) { return mhd_gpu_advance(h, 1, 1, st); }
+
+int mhd_gpu_state_device_ptr(mhd_gpu_t* h, int slot, double** dptr) {
+  if (!h || !dptr || slot < 0 || slot > h->R) return MHD_ERR_INVALID;
+  *dptr = h->u[slot];
+  return MHD_OK;
+}
+
+}  // extern "C"

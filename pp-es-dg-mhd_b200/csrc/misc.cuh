@@ -1,0 +1,268 @@
+// misc.cuh -- boundary fill, SSP-RK stage combination, layout transposes and the device-side
+// step control of solve_execute.
+#pragma once
+#include "common.cuh"
+
+namespace mhd {
+
+enum BcKind : int { BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_FIXED = 2, BC_XEXTRAP_YPER = 3 };
+
+// Ghost-ring fill (problems.f90:312-423,597-654).  One thread per ghost value; corners untouched.
+template <int P>
+__global__ void __launch_bounds__(256) bc_kernel(double* __restrict__ u, Geo g, const Ctrl* ctrl, int gate) {
+  constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
+  if (!gate_open(ctrl, gate)) return;
+  const int nx = g.nx, ny = g.ny, NXG = nx + 2;
+  const long long nghost = 2LL * (nx + ny);
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= nghost * EB) return;
+  const int ge = (int)(it / EB), vi = (int)(it - (long long)ge * EB);
+  const int v = vi / NN, q = vi - v * NN, k = q % N, l = q / N;
+  int i, j;        // ghost element
+  int si, sj, sq;  // source element and node
+  bool xside;      // left/right ghost column
+  if (ge < ny) { i = 0; j = 1 + ge; xside = true; }
+  else if (ge < 2 * ny) { i = nx + 1; j = 1 + ge - ny; xside = true; }
+  else if (ge < 2 * ny + nx) { i = 1 + ge - 2 * ny; j = 0; xside = false; }
+  else { i = 1 + ge - 2 * ny - nx; j = ny + 1; xside = false; }
+  const long long dst = ((long long)j * NXG + i) * EB + vi;
+  int kind = g.bc_kind;
+  if (kind == BC_XEXTRAP_YPER) kind = xside ? BC_EXTRAPOLATE : BC_PERIODIC;
+  if (kind == BC_FIXED) {
+    u[dst] = g.bc_state[v];
+    return;
+  }
+  if (kind == BC_PERIODIC) {
+    si = (i == 0) ? nx : (i == nx + 1 ? 1 : i);
+    sj = (j == 0) ? ny : (j == ny + 1 ? 1 : j);
+    sq = q;
+  } else {  // extrapolation of the adjacent interior trace
+    if (xside) {
+      si = (i == 0) ? 1 : nx;
+      sj = j;
+      sq = ((i == 0) ? 0 : N - 1) + N * l;
+    } else {
+      si = i;
+      sj = (j == 0) ? 1 : ny;
+      sq = k + N * ((j == 0) ? 0 : N - 1);
+    }
+  }
+  u[dst] = u[((long long)sj * NXG + si) * EB + v * NN + sq];
+}
+
+// SSP-RK stage update (drive.f90:130-275) on interior elements, rounded exactly as written
+// (explicit _rn intrinsics: no fused multiply-add contraction).
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+
+template <int EB>
+__global__ void __launch_bounds__(256)
+    combine_kernel(const double* __restrict__ u0, const double* __restrict__ r1, const double* __restrict__ r2,
+                   const double* __restrict__ r3, const double* __restrict__ r4,
+                   const double* __restrict__ k1, const double* __restrict__ k2, const double* __restrict__ k3,
+                   const double* __restrict__ k4, const double* __restrict__ k5, double* __restrict__ out,
+                   int nx, int ny, int R, int stage, const double* __restrict__ dt_ptr, double dt_arg,
+                   const Ctrl* ctrl, int gate) {
+  if (!gate_open(ctrl, gate)) return;
+  const long long n = (long long)nx * ny * EB;
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= n) return;
+  const double dt = dt_ptr ? *dt_ptr : dt_arg;
+  const long long e = it / EB;
+  const int c = (int)(it - e * EB);
+  const int j = 1 + (int)(e / nx), i = 1 + (int)(e - (long long)(j - 1) * nx);
+  const long long gi = ((long long)j * (nx + 2) + i) * EB + c;  // ghosted index
+  const long long ki = it;                                       // interior index
+  double val;
+  if (R == 1 || (stage == 1 && R <= 3)) {
+    val = add(u0[gi], mul(dt, k1[ki]));
+  } else if (R == 2) {
+    val = add(mul(0.5, u0[gi]), mul(0.5, add(r1[gi], mul(dt, k2[ki]))));
+  } else if (R == 3) {
+    if (stage == 2)
+      val = add(mul(0.75, u0[gi]), mul(0.25, add(r1[gi], mul(dt, k2[ki]))));
+    else
+      val = add(mul(1.0 / 3.0, u0[gi]), mul(2.0 / 3.0, add(r2[gi], mul(dt, k3[ki]))));
+  } else {  // SSP-RK(5,4)
+    switch (stage) {
+      case 1: val = add(u0[gi], mul(mul(0.391752226571890, dt), k1[ki])); break;
+      case 2: val = add(add(mul(0.444370493651235, u0[gi]), mul(0.555629506348765, r1[gi])), mul(mul(0.368410593050371, dt), k2[ki])); break;
+      case 3: val = add(add(mul(0.620101851488403, u0[gi]), mul(0.379898148511597, r2[gi])), mul(mul(0.251891774271694, dt), k3[ki])); break;
+      case 4: val = add(add(mul(0.178079954393132, u0[gi]), mul(0.821920045606868, r3[gi])), mul(mul(0.544974750228521, dt), k4[ki])); break;
+      default:
+        val = add(add(add(add(mul(0.517231671970585, r2[gi]), mul(0.096059710526147, r3[gi])), mul(mul(0.063692468666290, dt), k4[ki])),
+                      mul(0.386708617503269, r4[gi])), mul(mul(0.226007483236906, dt), k5[ki]));
+        break;
+    }
+  }
+  out[gi] = val;
+}
+
+// Fortran layout (8, n, n, E) <-> element-blocked layout [E][8][n*n].  E = element count.
+__global__ void __launch_bounds__(256) to_blocked_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                                        long long nelem, int NN) {
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = nelem * 8 * NN;
+  if (it >= n) return;
+  const int EB = 8 * NN;
+  const long long e = it / EB;
+  const int c = (int)(it - e * EB);
+  const int v = c / NN, q = c - v * NN;
+  dst[it] = src[e * EB + q * 8 + v];
+}
+__global__ void __launch_bounds__(256) to_fortran_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                                        long long nelem, int NN) {
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = nelem * 8 * NN;
+  if (it >= n) return;
+  const int EB = 8 * NN;
+  const long long e = it / EB;
+  const int c = (int)(it - e * EB);
+  const int q = c / 8, v = c - q * 8;
+  dst[it] = src[e * EB + v * NN + q];
+}
+
+// ---- device-side control of solve_execute (drive.f90:83-320) ---------------------------------
+
+__device__ __forceinline__ double dec_dtlim(unsigned long long b) { return __longlong_as_double((long long)b); }
+
+// reset the per-call outputs of post_process
+__global__ void ctl_pp_reset(Ctrl* c, int gate) {
+  if (!gate_open(c, gate)) return;
+  c->neg_avg = 0;
+  c->num_negcell = 0;
+  c->pp_relimit = 0;
+  for (int v = 0; v < 8; ++v) {
+    c->umax_bits[v] = 0ULL;
+    c->umin_bits[v] = ~0ULL;
+  }
+}
+
+// Fortran x**n for integer n >= 1 (binary exponentiation, as libgcc's __powidf2)
+__device__ __forceinline__ double powi_d(double x, int n) {
+  double r = (n & 1) ? x : 1.0;
+  while (n >>= 1) {
+    x = __dmul_rn(x, x);
+    if (n & 1) r = __dmul_rn(r, x);
+  }
+  return r;
+}
+
+// Start of one try of a time step (drive.f90:93-105).  Decodes the last residual's dt_lim.
+__global__ void ctl_step_begin(Ctrl* c) {
+  if (c->pending_dtlim) {
+    c->dt_lim = dec_dtlim(c->dt_lim_bits);
+    c->pending_dtlim = 0;
+  }
+  if (c->done || (c->flags & 0x6) || c->steps >= c->step_limit) {  // finished, error, or step budget used
+    c->state = ST_IDLE;
+    return;
+  }
+  c->try_num += 1;
+  if (c->try_num > 10 || c->dt_lim < 1e-14) {
+    c->flags |= 4;  // MHD_FLAG_DT_COLLAPSE
+    c->state = ST_IDLE;
+    return;
+  }
+  if (c->try_num > 1) {
+    c->retries += 1;
+    c->state = ST_RECOMPUTE;  // re-compute ut(:,1) from u_con (drive.f90:104)
+    c->dt_lim_bits = ~0ULL;
+    c->pending_dtlim = 1;
+  } else {
+    c->state = ST_RUN;
+  }
+}
+
+// dt of this try (drive.f90:107-120)
+__global__ void ctl_dt(Ctrl* c) {
+  if (c->pending_dtlim) {
+    c->dt_lim = dec_dtlim(c->dt_lim_bits);
+    c->pending_dtlim = 0;
+  }
+  if (c->state == ST_IDLE) return;
+  double dt;
+  if (c->try_num <= 1)
+    dt = __dmul_rn(c->cfl_total, c->dt_lim);
+  else
+    dt = __dmul_rn(powi_d(__dadd_rn(__dsqrt_rn(1.25), -0.5), c->try_num - 1), c->dt);
+  if (__dadd_rn(c->t, dt) >= c->final_T) {
+    dt = __dadd_rn(c->final_T, -c->t);
+    c->last_step = 1;
+  } else {
+    c->last_step = 0;
+  }
+  c->dt = dt;
+  c->state = ST_RUN;
+}
+
+// pseudo-time of stage s (drive.f90:142-267), computed before the stage's combine
+__global__ void ctl_stage_time(Ctrl* c, int R, int s) {
+  if (c->state != ST_RUN) return;
+  const double t = c->t, dt = c->dt;
+  double* tr = c->t_rk;
+  double v;
+  if (R == 1 || (s == 1 && R <= 3)) v = __dadd_rn(t, __dmul_rn(dt, 1.0));
+  else if (R == 2) v = __dadd_rn(__dmul_rn(0.5, t), __dmul_rn(0.5, __dadd_rn(tr[1], __dmul_rn(dt, 1.0))));
+  else if (R == 3)
+    v = (s == 2) ? __dadd_rn(__dmul_rn(0.75, t), __dmul_rn(0.25, __dadd_rn(tr[1], __dmul_rn(dt, 1.0))))
+                 : __dadd_rn(__dmul_rn(1.0 / 3.0, t), __dmul_rn(2.0 / 3.0, __dadd_rn(tr[2], __dmul_rn(dt, 1.0))));
+  else {
+    switch (s) {
+      case 1: v = __dadd_rn(t, __dmul_rn(__dmul_rn(0.391752226571890, dt), 1.0)); break;
+      case 2: v = __dadd_rn(__dadd_rn(__dmul_rn(0.444370493651235, t), __dmul_rn(0.555629506348765, tr[1])), __dmul_rn(__dmul_rn(0.368410593050371, dt), 1.0)); break;
+      case 3: v = __dadd_rn(__dadd_rn(__dmul_rn(0.620101851488403, t), __dmul_rn(0.379898148511597, tr[2])), __dmul_rn(__dmul_rn(0.251891774271694, dt), 1.0)); break;
+      case 4: v = __dadd_rn(__dadd_rn(__dmul_rn(0.178079954393132, t), __dmul_rn(0.821920045606868, tr[3])), __dmul_rn(__dmul_rn(0.544974750228521, dt), 1.0)); break;
+      default:
+        v = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.517231671970585, tr[2]), __dmul_rn(0.096059710526147, tr[3])),
+                                          __dmul_rn(__dmul_rn(0.063692468666290, dt), 1.0)),
+                                __dmul_rn(0.386708617503269, tr[4])),
+                      __dmul_rn(__dmul_rn(0.226007483236906, dt), 1.0));
+        break;
+    }
+  }
+  tr[s] = v;
+  // reset the post_process outputs of this stage
+  c->neg_avg = 0;
+  c->num_negcell = 0;
+  c->pp_relimit = 0;
+  for (int v8 = 0; v8 < 8; ++v8) {
+    c->umax_bits[v8] = 0ULL;
+    c->umin_bits[v8] = ~0ULL;
+  }
+}
+
+// after post_process of a stage (drive.f90:285-298): inadmissible average -> abandon the try;
+// otherwise account the limiter count and arm the dt_lim reduction of the coming residual.
+__global__ void ctl_stage_end(Ctrl* c) {
+  if (c->state != ST_RUN) return;
+  if (c->pp_relimit) {
+    c->flags |= 2;  // MHD_FLAG_PP_RELIMIT (the reference stops the program)
+    c->state = ST_IDLE;
+    return;
+  }
+  if (c->neg_avg) {
+    c->state = ST_FAILED;
+    return;
+  }
+  c->num_negcell_last = c->num_negcell;
+  c->num_negcell_total += c->num_negcell;
+  c->dt_lim_bits = ~0ULL;
+  c->pending_dtlim = 1;
+}
+
+// end of a try: accept (drive.f90:304-312) or prepare the re-try
+__global__ void ctl_step_end(Ctrl* c, int R) {
+  if (c->state == ST_FAILED) {  // re-try with a smaller dt
+    c->state = ST_IDLE;
+    return;
+  }
+  if (c->state != ST_RUN) return;
+  c->t = c->t_rk[R];
+  c->steps += 1;
+  c->try_num = 0;
+  if (c->last_step) c->done = 1;
+  c->state = ST_IDLE;
+}
+
+}  // namespace mhd

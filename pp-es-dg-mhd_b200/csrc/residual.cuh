@@ -1,0 +1,383 @@
+// residual.cuh -- DG_semidiscretize (DG_solver.f90:663-892) as one sm_100a kernel.
+//
+// One CTA owns a TX x TY tile of interior elements.  Phases (separated by __syncthreads):
+//   0  load: tile rows are contiguous runs of element blocks -> 128-bit loads into shared
+//      memory; the four halo traces (the neighbour nodes on the tile boundary) come from the
+//      neighbouring elements (ghost ring or the next tile).
+//   1  per node: primitives (rho, v, B, beta) and the fast wave speeds.
+//   2  fluxes: every interface node of the tile gets ESPP_HLL_flux_x once (the y faces through
+//      swap_xy), and every element node pair along x and y gets its entropy-conservative flux
+//      once (the reference's symmetric r<k / s<l scatter, DG_solver.f90:833-848).
+//   3  per node: diagonal volume term, Godunov-Powell source with the local div B, the pair
+//      contributions in a fixed order, and the surface terms; per element: dt_lim.
+//   4  store: ut tile rows back with 128-bit stores; block min of dt_lim -> one atomicMin.
+// Work items of a phase are spread over the CTA's threads round-robin.  Sums are formed in a
+// fixed order, so the kernel is deterministic.
+#pragma once
+#include "common.cuh"
+
+namespace mhd {
+
+template <int P>
+struct ResCfg;
+template <>
+struct ResCfg<1> { static constexpr int TX = 8, TY = 8, NT = 256; };
+template <>
+struct ResCfg<2> { static constexpr int TX = 4, TY = 4, NT = 256; };
+template <>
+struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 256; };
+
+template <int P>
+struct ResLayout {
+  static constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
+  static constexpr int TX = ResCfg<P>::TX, TY = ResCfg<P>::TY, TE = TX * TY;
+  static constexpr int NPR = N * (N - 1) / 2;  // pairs per line
+  static constexpr int NPX = N * NPR;          // x pairs per element
+  static constexpr int NPAIR = 2 * NPX;
+  static constexpr int NFX = (TX + 1) * TY * N;
+  static constexpr int NFY = TX * (TY + 1) * N;
+  static constexpr int FW = 11;  // face record: flux[8], nB, sl, sr
+  // offsets in doubles
+  static constexpr int O_CONS = 0;
+  static constexpr int O_PRIM = O_CONS + TE * EB;
+  static constexpr int O_HXL = O_PRIM + TE * EB;
+  static constexpr int O_HXR = O_HXL + TY * 8 * N;
+  static constexpr int O_HYB = O_HXR + TY * 8 * N;
+  static constexpr int O_HYT = O_HYB + TX * 8 * N;
+  static constexpr int O_FX = O_HYT + TX * 8 * N;
+  static constexpr int O_FY = O_FX + NFX * FW;
+  static constexpr int O_PAIR = O_FY + NFY * FW;
+  static constexpr int O_SIG = O_PAIR + TE * NPAIR * 8;
+  static constexpr int O_RED = O_SIG + TE * 2 * NN;
+  static constexpr int TOTAL = O_RED + 32;
+  static constexpr size_t BYTES = sizeof(double) * TOTAL;
+};
+
+// pair index within a line -> (a, b), b < a, enumerated a = 1..N-1, b = 0..a-1
+__device__ __forceinline__ void pair_ab(int idx, int& a, int& b) {
+  a = 1;
+  while (idx >= a) {
+    idx -= a;
+    ++a;
+  }
+  b = idx;
+}
+__device__ __forceinline__ int pair_index(int a, int b) { return a * (a - 1) / 2 + b; }
+
+template <int P>
+__global__ void __launch_bounds__(ResCfg<P>::NT, 1)
+    residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl,
+                    int gate) {
+  using L = ResLayout<P>;
+  constexpr int N = L::N, NN = L::NN, EB = L::EB, TX = L::TX, TY = L::TY, TE = L::TE;
+  constexpr int NT = ResCfg<P>::NT;
+  if (!gate_open(ctrl, gate)) return;
+  extern __shared__ __align__(16) double sm[];
+  double* s_cons = sm + L::O_CONS;
+  double* s_prim = sm + L::O_PRIM;
+  double* s_hxl = sm + L::O_HXL;
+  double* s_hxr = sm + L::O_HXR;
+  double* s_hyb = sm + L::O_HYB;
+  double* s_hyt = sm + L::O_HYT;
+  double* s_fx = sm + L::O_FX;
+  double* s_fy = sm + L::O_FY;
+  double* s_pair = sm + L::O_PAIR;
+  double* s_sig = sm + L::O_SIG;
+  double* s_red = sm + L::O_RED;
+
+  const int tid = threadIdx.x;
+  const int nx = g.nx, ny = g.ny;
+  const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;  // first interior element
+  const int W = min(TX, nx - i0 + 1), H = min(TY, ny - j0 + 1);
+  const long long rowstride = (long long)(nx + 2) * EB;
+  const double gamma = g.gamma;
+
+  // ---- phase 0: load the tile and its halo traces ----
+  {
+    constexpr int V2 = TX * EB / 2;  // double2 per tile row
+    for (int it = tid; it < H * V2; it += NT) {
+      const int r = it / V2, c = it - r * V2;
+      if (c < W * EB / 2) {
+        const double2* src = reinterpret_cast<const double2*>(u + (long long)(j0 + r) * rowstride + (long long)i0 * EB);
+        reinterpret_cast<double2*>(s_cons + r * TX * EB)[c] = __ldg(src + c);
+      }
+    }
+    for (int it = tid; it < TY * 8 * N; it += NT) {  // x halos: traces k = n-1 (left) / 0 (right)
+      const int r = it / (8 * N), rem = it - r * 8 * N, v = rem / N, l = rem - v * N;
+      if (r < H) {
+        const double* rowp = u + (long long)(j0 + r) * rowstride;
+        s_hxl[it] = __ldg(rowp + (long long)(i0 - 1) * EB + v * NN + (N - 1) + N * l);
+        s_hxr[it] = __ldg(rowp + (long long)(i0 + W) * EB + v * NN + 0 + N * l);
+      }
+    }
+    for (int it = tid; it < TX * 8 * N; it += NT) {  // y halos: traces l = n-1 (bottom) / 0 (top)
+      const int c = it / (8 * N), rem = it - c * 8 * N, v = rem / N, k = rem - v * N;
+      if (c < W) {
+        s_hyb[it] = __ldg(u + (long long)(j0 - 1) * rowstride + (long long)(i0 + c) * EB + v * NN + k + N * (N - 1));
+        s_hyt[it] = __ldg(u + (long long)(j0 + H) * rowstride + (long long)(i0 + c) * EB + v * NN + k);
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 1: primitives and node wave speeds ----
+  for (int it = tid; it < TE * NN; it += NT) {
+    const int e = it / NN, q = it - e * NN;
+    const int er = e / TX, ec = e - er * TX;
+    if (er >= H || ec >= W) continue;
+    const double* w0 = s_cons + e * EB + q;
+    double w[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) w[v] = w0[v * NN];
+    const double ir = 1.0 / w[0];
+    const double vx = ir * w[1], vy = ir * w[2], vz = ir * w[3];
+    const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+    const double bsq = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
+    const double pf = fmax((gamma - 1.0) * (w[7] - (ek + 0.5 * bsq)), PP_EPS);
+    double* pr = s_prim + e * EB + q;
+    pr[0 * NN] = w[0];
+    pr[1 * NN] = vx;
+    pr[2 * NN] = vy;
+    pr[3 * NN] = vz;
+    pr[4 * NN] = w[4];
+    pr[5 * NN] = w[5];
+    pr[6 * NN] = w[6];
+    pr[7 * NN] = 0.5 * w[0] / pf;
+    const double cs = gamma * pf * ir, ss = cs + bsq * ir, coef = 4.0 * cs * ir;
+    s_sig[e * 2 * NN + q] = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
+    s_sig[e * 2 * NN + NN + q] = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
+  }
+  __syncthreads();
+
+  // ---- phase 2: interface fluxes and element pair fluxes ----
+  {
+    constexpr int NITEM = L::NFX + L::NFY + TE * L::NPAIR;
+    for (int it = tid; it < NITEM; it += NT) {
+      if (it < L::NFX) {  // x face node
+        const int fi = it / (TY * N), rem = it - fi * TY * N, r = rem / N, l = rem - r * N;
+        if (r >= H || fi > W) continue;
+        double wl[8], wr[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          wl[v] = (fi == 0) ? s_hxl[(r * 8 + v) * N + l] : s_cons[(r * TX + fi - 1) * EB + v * NN + (N - 1) + N * l];
+          wr[v] = (fi == W) ? s_hxr[(r * 8 + v) * N + l] : s_cons[(r * TX + fi) * EB + v * NN + N * l];
+        }
+        espp_hll(wl, wr, gamma, s_fx + it * L::FW);
+      } else if (it < L::NFX + L::NFY) {  // y face node (swap_xy in and out)
+        const int f = it - L::NFX;
+        const int fj = f / (TX * N), rem = f - fj * TX * N, c = rem / N, k = rem - c * N;
+        if (c >= W || fj > H) continue;
+        double a[8], b[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          a[v] = (fj == 0) ? s_hyb[(c * 8 + v) * N + k] : s_cons[((fj - 1) * TX + c) * EB + v * NN + k + N * (N - 1)];
+          b[v] = (fj == H) ? s_hyt[(c * 8 + v) * N + k] : s_cons[(fj * TX + c) * EB + v * NN + k];
+        }
+        double sa[8] = {a[0], a[2], a[1], a[3], a[5], a[4], a[6], a[7]};
+        double sb[8] = {b[0], b[2], b[1], b[3], b[5], b[4], b[6], b[7]};
+        double o[11];
+        espp_hll(sa, sb, gamma, o);
+        double* dst = s_fy + f * L::FW;
+        dst[0] = o[0];
+        dst[1] = o[2];
+        dst[2] = o[1];
+        dst[3] = o[3];
+        dst[4] = o[5];
+        dst[5] = o[4];
+        dst[6] = o[6];
+        dst[7] = o[7];
+        dst[8] = o[8];
+        dst[9] = o[9];
+        dst[10] = o[10];
+      } else {  // element node pair
+        const int pidx = it - L::NFX - L::NFY;
+        const int e = pidx / L::NPAIR, pi = pidx - e * L::NPAIR;
+        const int er = e / TX, ec = e - er * TX;
+        if (er >= H || ec >= W) continue;
+        const double* pb = s_prim + e * EB;
+        double A[8], B[8], F[8];
+        if (pi < L::NPX) {  // x pair on line l: nodes (a,l) [the reference's k] and (b,l) [r]
+          const int l = pi / L::NPR;
+          int a, b;
+          pair_ab(pi - l * L::NPR, a, b);
+#pragma unroll
+          for (int v = 0; v < 8; ++v) {
+            A[v] = pb[v * NN + a + N * l];
+            B[v] = pb[v * NN + b + N * l];
+          }
+          ec_flux<0>(A, B, gamma, F);
+        } else {  // y pair on column k: nodes (k,a) [the reference's l] and (k,b) [s]
+          const int pj = pi - L::NPX;
+          const int k = pj / L::NPR;
+          int a, b;
+          pair_ab(pj - k * L::NPR, a, b);
+#pragma unroll
+          for (int v = 0; v < 8; ++v) {
+            A[v] = pb[v * NN + k + N * a];
+            B[v] = pb[v * NN + k + N * b];
+          }
+          ec_flux<1>(A, B, gamma, F);
+        }
+        double* dst = s_pair + (e * L::NPAIR + pi) * 8;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) dst[v] = F[v];
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 3: assemble ut per node; dt_lim per element ----
+  const DegConst& dc = c_deg[P];
+  const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
+  double my_dt = 1.0e300;
+  for (int it = tid; it < TE * NN + TE; it += NT) {
+    if (it < TE * NN) {
+      const int e = it / NN, q = it - e * NN;
+      const int er = e / TX, ec = e - er * TX;
+      if (er >= H || ec >= W) continue;
+      const int k = q % N, l = q / N;
+      double* cw = s_cons + e * EB + q;
+      const double* pb = s_prim + e * EB;
+      double w[8];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) w[v] = cw[v * NN];
+      // node flux F, G and Godunov-Powell coefficients (DG_solver.f90:749-799)
+      const double ir = 1.0 / w[0];
+      const double vx = ir * w[1], vy = ir * w[2], vz = ir * w[3];
+      const double bx = w[4], by = w[5], bz = w[6];
+      const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+      const double bsq = bx * bx + by * by + bz * bz;
+      const double pm = 0.5 * bsq;
+      const double pf = fmax((gamma - 1.0) * (w[7] - (ek + pm)), PP_EPS);
+      const double pt = pf + pm;
+      const double bu = bx * vx + by * vy + bz * vz;
+      const double ex = by * vz - bz * vy, ey = bz * vx - bx * vz, ez = bx * vy - by * vx;
+      double F[8], G[8], GP[8];
+      F[0] = w[1];
+      F[1] = vx * w[1] - bx * bx + pt;
+      F[2] = vx * w[2] - by * bx;
+      F[3] = vx * w[3] - bz * bx;
+      F[4] = 0.0;
+      F[5] = -ez;
+      F[6] = ey;
+      F[7] = vx * (w[7] + pt) - bx * bu;
+      G[0] = w[2];
+      G[1] = vy * w[1] - bx * by;
+      G[2] = vy * w[2] - by * by + pt;
+      G[3] = vy * w[3] - bz * by;
+      G[4] = ez;
+      G[5] = 0.0;
+      G[6] = -ex;
+      G[7] = vy * (w[7] + pt) - by * bu;
+      GP[0] = 0.0;
+      GP[1] = bx;
+      GP[2] = by;
+      GP[3] = bz;
+      GP[4] = vx;
+      GP[5] = vy;
+      GP[6] = vz;
+      GP[7] = bu;
+      // local div B (DG_solver.f90:813)
+      double dbx = 0.0, dby = 0.0;
+#pragma unroll
+      for (int r = 0; r < N; ++r) dbx += dc.D[k + N * r] * pb[4 * NN + r + N * l];
+#pragma unroll
+      for (int m = 0; m < N; ++m) dby += pb[5 * NN + k + N * m] * dc.D[l + N * m];
+      const double divB = sxh * dbx + syh * dby;
+      double acc[8];
+      const double ckk = 2.0 * sxh * dc.D[k + N * k], cll = 2.0 * syh * dc.D[l + N * l];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) acc[v] = -(ckk * F[v]) - cll * G[v] - divB * GP[v];
+      // pair contributions along x (line l) and y (column k)
+      const double* pe = s_pair + e * L::NPAIR * 8;
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        if (r == k) continue;
+        const int pi = l * L::NPR + pair_index(max(k, r), min(k, r));
+        const double c = 2.0 * sxh * dc.D[k + N * r];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[pi * 8 + v];
+      }
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        if (m == l) continue;
+        const int pi = L::NPX + k * L::NPR + pair_index(max(l, m), min(l, m));
+        const double c = 2.0 * syh * dc.D[l + N * m];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[pi * 8 + v];
+      }
+      // surface terms (DG_solver.f90:872-882)
+      if (k == 0) {
+        const double* fr = s_fx + ((ec * TY + er) * N + l) * L::FW;
+        const double c = sxh / dc.qw[0];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] -= c * (F[v] - fr[v] + GP[v] * (bx - fr[8]));
+      }
+      if (k == N - 1) {
+        const double* fr = s_fx + (((ec + 1) * TY + er) * N + l) * L::FW;
+        const double c = sxh / dc.qw[N - 1];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v] + GP[v] * (bx - fr[8]));
+      }
+      if (l == 0) {
+        const double* fr = s_fy + ((er * TX + ec) * N + k) * L::FW;
+        const double c = syh / dc.qw[0];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] -= c * (G[v] - fr[v] + GP[v] * (by - fr[8]));
+      }
+      if (l == N - 1) {
+        const double* fr = s_fy + (((er + 1) * TX + ec) * N + k) * L::FW;
+        const double c = syh / dc.qw[N - 1];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v] + GP[v] * (by - fr[8]));
+      }
+#pragma unroll
+      for (int v = 0; v < 8; ++v) cw[v * NN] = acc[v];  // own node only: safe in place
+    } else {
+      const int e = it - TE * NN;
+      const int er = e / TX, ec = e - er * TX;
+      if (er >= H || ec >= W) continue;
+      double sx = 0.0, sy = 0.0;
+      for (int q = 0; q < NN; ++q) {
+        sx = fmax(sx, s_sig[e * 2 * NN + q]);
+        sy = fmax(sy, s_sig[e * 2 * NN + NN + q]);
+      }
+      double mxr = -1.0e300, mnl = 1.0e300, myu = -1.0e300, mnd = 1.0e300;
+      for (int l = 0; l < N; ++l) {
+        mxr = fmax(mxr, s_fx[((ec * TY + er) * N + l) * L::FW + 10]);
+        mnl = fmin(mnl, s_fx[(((ec + 1) * TY + er) * N + l) * L::FW + 9]);
+      }
+      for (int k = 0; k < N; ++k) {
+        myu = fmax(myu, s_fy[((er * TX + ec) * N + k) * L::FW + 10]);
+        mnd = fmin(mnd, s_fy[(((er + 1) * TX + ec) * N + k) * L::FW + 9]);
+      }
+      const double ax = fmax(fmax(sx, mxr), -mnl), ay = fmax(fmax(sy, myu), -mnd);
+      const double dtl = 1.0 / ((2 * P + 1) * ax / g.hx + (2 * P + 1) * ay / g.hy);
+      my_dt = fmin(my_dt, dtl);
+    }
+  }
+  // block min of dt_lim
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) my_dt = fmin(my_dt, __shfl_xor_sync(0xffffffffu, my_dt, o));
+  if ((tid & 31) == 0) s_red[tid >> 5] = my_dt;
+  __syncthreads();
+  if (tid == 0) {
+    double m = s_red[0];
+    for (int w = 1; w < NT / 32; ++w) m = fmin(m, s_red[w]);
+    atomicMin(&ctrl->dt_lim_bits, (unsigned long long)__double_as_longlong(m));
+  }
+
+  // ---- phase 4: store ut ----
+  {
+    constexpr int V2 = TX * EB / 2;
+    for (int it = tid; it < H * V2; it += NT) {
+      const int r = it / V2, c = it - r * V2;
+      if (c < W * EB / 2) {
+        double2* dst = reinterpret_cast<double2*>(ut + ((long long)(j0 + r - 1) * nx + (i0 - 1)) * EB);
+        dst[c] = reinterpret_cast<const double2*>(s_cons + r * TX * EB)[c];
+      }
+    }
+  }
+}
+
+}  // namespace mhd

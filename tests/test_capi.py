@@ -1,0 +1,54 @@
+"""The C-ABI library loads and exports every function include/mhd_gpu.h declares (CPU, no GPU compute)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from conftest import ROOT
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "mhd_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(mhd_gpu_\w+)\s*\(", src)))
+
+
+def test_every_declared_symbol_is_exported(pkg):
+    lib = C.CDLL(pkg.capi.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # the Python binding declares exactly the header's functions
+    assert sorted(pkg.capi.SIGNATURES) == names
+
+
+def test_status_strings(pkg):
+    cap = pkg.capi
+    assert cap.status_string(0) == "ok"
+    assert "average" in cap.status_string(cap.MHD_FLAG_NEG_AVG)
+    assert "CUDA" in cap.status_string(cap.MHD_ERR_CUDA)
+
+
+def test_host_only_entry_points(pkg):
+    lib = pkg.capi.load()
+    dp = C.POINTER(C.c_double)
+    x = np.zeros(4)
+    assert lib.mhd_gpu_gll_tables(3, x.ctypes.data_as(dp), None, None, None, None, None, None) == 0
+    assert lib.mhd_gpu_gll_tables(7, x.ctypes.data_as(dp), None, None, None, None, None, None) < 0
+    A = np.zeros((32, 32))
+    assert lib.mhd_gpu_ldf_operator(3, 0.1, 0.1, A.ctypes.data_as(dp)) == 0
+    assert lib.mhd_gpu_ldf_operator(3, -0.1, 0.1, A.ctypes.data_as(dp)) < 0
+
+
+def test_create_rejects_bad_arguments_before_touching_a_device(pkg):
+    lib = pkg.capi.load()
+    h = C.c_void_p()
+    # unsupported degree / unequal degrees / bad rknstg / bad domain
+    assert lib.mhd_gpu_create(8, 8, 4, 4, 3, 0.0, 1.0, 0.0, 1.0, 1.4, 0, None, C.byref(h)) == pkg.capi.MHD_ERR_UNSUPPORTED
+    assert lib.mhd_gpu_create(8, 8, 2, 1, 3, 0.0, 1.0, 0.0, 1.0, 1.4, 0, None, C.byref(h)) == pkg.capi.MHD_ERR_UNSUPPORTED
+    assert lib.mhd_gpu_create(8, 8, 2, 2, 4, 0.0, 1.0, 0.0, 1.0, 1.4, 0, None, C.byref(h)) == pkg.capi.MHD_ERR_UNSUPPORTED
+    assert lib.mhd_gpu_create(8, 8, 2, 2, 3, 1.0, 0.0, 0.0, 1.0, 1.4, 0, None, C.byref(h)) == pkg.capi.MHD_ERR_INVALID
+    assert lib.mhd_gpu_create(8, 8, 2, 2, 3, 0.0, 1.0, 0.0, 1.0, 1.4, 2, None, C.byref(h)) == pkg.capi.MHD_ERR_INVALID
+    assert not h.value

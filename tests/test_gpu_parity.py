@@ -1,0 +1,188 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle on the same inputs.
+
+Tolerances (FP64):
+  * residual ut, post-processed states, one SSP-RK3 step: relative L1 per conserved variable
+    <= 1e-12 (the north-star parity bar; observed differences are at the 1e-15 level, from FMA
+    contraction and libm vs CUDA log/exp/sqrt rounding);
+  * dt_lim, tot_ent: relative 1e-13;
+  * integer outputs (neg_avg, num_negcell, retries, steps): exact.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l1
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _setup(pkg, ora, name, nx, ny, p, amp=1.0, rknstg=3):
+    prob = pkg.problems.make(name, amp=amp)
+    u0 = prob.initial_state(nx, ny, p)
+    g = pkg.DGSolver.for_problem(prob, nx, ny, p, rknstg)
+    o = ora.OracleSolver(nx, ny, p, p, rknstg, *prob.domain, prob.gamma, prob.bc_kind, prob.bc_state)
+    return prob, u0, g, o
+
+
+def _perturbed(u0, seed, scale=0.02):
+    """interior perturbed by a smooth-ish random field that keeps density/pressure positive"""
+    rng = np.random.default_rng(seed)
+    u = u0.copy()
+    inner = u[:, :, :, 1:-1, 1:-1]
+    noise = rng.standard_normal(inner.shape)
+    inner[1:7] += scale * noise[1:7] * (1.0 + np.abs(inner[1:7]))
+    inner[0] *= 1.0 + 0.5 * scale * np.tanh(noise[0])
+    inner[7] *= 1.0 + 2.0 * scale + 0.5 * scale * np.tanh(noise[7])
+    return u
+
+
+CASES = [("ot2pi", 8, 8, 1), ("ot2pi", 12, 10, 2), ("ot2pi", 9, 7, 3), ("blast", 10, 12, 2),
+         ("rotor", 11, 9, 2), ("vortex", 10, 10, 3), ("ot_unit", 17, 13, 1)]
+
+
+@pytest.mark.parametrize("name,nx,ny,p", CASES)
+def test_residual_parity(pkg, ora, name, nx, ny, p):
+    prob, u0, g, o = _setup(pkg, ora, name, nx, ny, p)
+    u = _perturbed(u0, seed=nx * 31 + p)
+    # ghosts by the solver's own BC on both sides
+    g.upload_state(0, u)
+    g.apply_bc(0)
+    ug = g.download_state(0)
+    uo = np.asfortranarray(u.copy())
+    o.apply_bc(uo)
+    inner_ghost = np.isfinite(uo)
+    assert np.array_equal(np.isfinite(ug), inner_ghost)
+    assert np.array_equal(ug[inner_ghost], uo[inner_ghost]), "BC fill must be bit-exact"
+    dl_g = g.semidiscretize(1, 0)
+    ut_g = g.download_ut(1)
+    ut_o, dl_o = o.semidiscretize(uo)
+    err = rel_l1(ut_g, ut_o)
+    assert err.max() <= TOL, err
+    assert abs(dl_g - dl_o) <= 1e-13 * dl_o
+    g.close()
+
+
+@pytest.mark.parametrize("name,nx,ny,p", CASES)
+@pytest.mark.parametrize("oedg,ldf,comput_ent,ent_offset", [(0, 1, 1, 0), (1, 1, 1, 0), (1, 0, 0, 0),
+                                                           (0, 0, 1, 1), (1, 1, 1, 1)])
+def test_post_process_parity(pkg, ora, name, nx, ny, p, oedg, ldf, comput_ent, ent_offset):
+    prob, u0, g, o = _setup(pkg, ora, name, nx, ny, p)
+    # the blast's low pressure (0.1) under B ~ 28 tolerates only small field perturbations
+    u = _perturbed(u0, seed=nx + 7 * p, scale=0.002 if name == "blast" else 0.05)
+    uo = np.asfortranarray(u.copy())
+    o.apply_bc(uo)
+    g.upload_state(0, uo)
+    avg_o = np.full((8, nx + 2, ny + 2), np.nan, order="F")
+    ro = o.post_process(uo, avg_o, oedg, ldf, 1.3e-3, ent_offset, comput_ent)
+    rg = g.post_process(0, oedg, ldf, 1.3e-3, ent_offset, comput_ent)
+    assert rg["neg_avg"] == ro["neg_avg"]
+    assert not ro["neg_avg"], "case must stay admissible"
+    assert rg["num_negcell"] == ro["num_negcell"]
+    if comput_ent and not ro["neg_avg"]:
+        assert abs(rg["tot_ent"] - ro["tot_ent"]) <= 1e-13 * abs(ro["tot_ent"])
+    else:
+        assert np.isnan(rg["tot_ent"]) and np.isnan(ro["tot_ent"])
+    ug = g.download_state(0)
+    m = np.isfinite(uo)
+    err = rel_l1(np.where(m, ug, 0.0), np.where(m, uo, 0.0))
+    assert err.max() <= TOL, err
+    ag = g.download_avg()
+    ma = np.isfinite(avg_o)
+    assert rel_l1(np.where(ma, ag, 0), np.where(ma, avg_o, 0)).max() <= TOL
+    g.close()
+
+
+def test_inadmissible_average_flag(pkg, ora):
+    """a state with negative cell averages: both report neg_avg (the state itself is then
+    unspecified, because the step is discarded) and neither reports an entropy"""
+    prob, u0, g, o = _setup(pkg, ora, "blast", 10, 12, 2)
+    u = _perturbed(u0, seed=27, scale=0.05)
+    uo = np.asfortranarray(u.copy())
+    o.apply_bc(uo)
+    g.upload_state(0, uo)
+    avg_o = np.full((8, 12, 14), np.nan, order="F")
+    ro = o.post_process(uo, avg_o, 1, 1, 1e-3, 0, 1)
+    rg = g.post_process(0, 1, 1, 1e-3, 0, 1)
+    assert ro["neg_avg"] and rg["neg_avg"]
+    assert rg["num_negcell"] == ro["num_negcell"] == 0
+    assert np.isnan(rg["tot_ent"]) and np.isnan(ro["tot_ent"])
+    g.close()
+
+
+@pytest.mark.parametrize("name,nx,ny,p", CASES)
+@pytest.mark.parametrize("rknstg", [3])
+def test_one_step_parity(pkg, ora, name, nx, ny, p, rknstg):
+    """after one SSP-RK3 step: relative L1 <= 1e-12 per conserved variable"""
+    prob, u0, g, o = _setup(pkg, ora, name, nx, ny, p, rknstg=rknstg)
+    sg = g.solve_execute(u0, prob.final_T, prob.cfl, max_steps=1)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, prob.cfl, max_steps=1)
+    assert so["status"] == 0 and sg["flags"] == 0
+    assert sg["steps"] == so["steps"] == 1
+    assert sg["retries"] == so["retries"]
+    assert abs(sg["t"] - so["t"]) <= 1e-14 * so["t"]
+    assert abs(sg["dt_lim"] - so["dt_lim"]) <= 1e-13 * so["dt_lim"]
+    ug = g.download_state(0)[:, :, :, 1:-1, 1:-1]
+    uo = o.u_con[:, :, :, 1:-1, 1:-1]
+    err = rel_l1(ug, uo)
+    assert err.max() <= TOL, err
+    g.close()
+
+
+@pytest.mark.parametrize("rknstg", [1, 2, 5])
+def test_other_rk_schemes(pkg, ora, rknstg):
+    prob, u0, g, o = _setup(pkg, ora, "ot2pi", 10, 10, 2, rknstg=rknstg)
+    sg = g.solve_execute(u0, prob.final_T, 0.1, max_steps=3)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, 0.1, max_steps=3)
+    assert sg["steps"] == so["steps"] == 3
+    err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+    assert err.max() <= 1e-12, err
+    g.close()
+
+
+def test_multi_step_blast_limiter_counts(pkg, ora):
+    """blast: the PP limiter is active; limiter counts and states follow the oracle"""
+    prob, u0, g, o = _setup(pkg, ora, "blast", 24, 24, 2)
+    sg = g.solve_execute(u0, prob.final_T, prob.cfl, max_steps=10)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, prob.cfl, max_steps=10)
+    assert sg["steps"] == so["steps"] == 10
+    assert sg["retries"] == so["retries"]
+    assert sg["num_negcell_total"] == so["num_negcell_total"]
+    err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+    assert err.max() <= 1e-11, err
+    ug = g.download_state(0)[:, :, :, 1:-1, 1:-1]
+    assert ug[0].min() > 0
+    g.close()
+
+
+def test_retry_path(pkg, ora):
+    """an over-large CFL makes an average inadmissible; both re-try with the golden-ratio shrink"""
+    prob, u0, g, o = _setup(pkg, ora, "blast", 16, 16, 2)
+    cfl = 10.0
+    sg = g.solve_execute(u0, prob.final_T, cfl, max_steps=4)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, cfl, max_steps=4)
+    assert so["retries"] > 0
+    assert sg["retries"] == so["retries"]
+    assert sg["steps"] == so["steps"]
+    assert abs(sg["t"] - so["t"]) <= 1e-13 * so["t"]
+    err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+    assert err.max() <= 1e-11, err
+    g.close()
+
+
+def test_ot_full_run_small(pkg, ora):
+    """Orszag-Tang 16x16 p=2 to t=0.5 (the plain-method config shape on a small mesh)"""
+    prob, u0, g, o = _setup(pkg, ora, "ot2pi", 16, 16, 2)
+    sg = g.solve_execute(u0, prob.final_T, prob.cfl)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, prob.cfl)
+    assert sg["done"] == 1 and sg["steps"] == so["steps"]
+    assert sg["t"] == so["t"]
+    err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+    assert err.max() <= 1e-10, err
+    assert abs(sg["tot_ent"] - so["tot_ent"]) <= 1e-12 * abs(so["tot_ent"])
+    g.close()

@@ -1,0 +1,99 @@
+"""Solver-level invariants of the oracle and checks of the host set-ups (CPU).
+
+* mass is conserved to round-off on periodic domains (the limiters keep cell averages and the
+  Godunov-Powell source has no density component);
+* density and pressure stay positive and the discrete entropy does not increase (blast, OT);
+* the vortex initial condition is a steady state in the co-moving frame: the residual of the
+  vortex with zero bulk velocity converges to zero under refinement;
+* the re-try path (drive.f90:93-116) engages on an over-large CFL and still finishes admissibly.
+"""
+import numpy as np
+import pytest
+
+
+def integral(u, w):
+    W = 0.25 * np.outer(w, w)
+    return np.einsum("sklij,kl->s", u[:, :, :, 1:-1, 1:-1], W)
+
+
+def make(pkg, ora, name, n, p, **kw):
+    prob = pkg.problems.make(name, **kw)
+    u0 = prob.initial_state(n, n, p)
+    o = ora.OracleSolver(n, n, p, p, 3, *prob.domain, prob.gamma, prob.bc_kind, prob.bc_state)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    return prob, u0, o
+
+
+def test_mass_conservation_ot(pkg, ora):
+    prob, u0, o = make(pkg, ora, "ot2pi", 12, 2)
+    w = ora.gll_tables(2)["w"]
+    m0 = integral(o.u_con.copy(), w)
+    r = o.solve(prob.final_T, prob.cfl, max_steps=25)
+    assert r["status"] == 0 and r["steps"] == 25
+    m1 = integral(o.u_con, w)
+    assert abs(m1[0] - m0[0]) <= 1e-13 * abs(m0[0])
+
+
+def test_entropy_decreases_and_positivity_blast(pkg, ora):
+    prob, u0, o = make(pkg, ora, "blast", 20, 2)
+    ents = []
+    r0 = o.solve(prob.final_T, prob.cfl, max_steps=1)
+    ents.append(r0["tot_ent"])
+    for _ in range(6):
+        r = o.solve(prob.final_T, prob.cfl, max_steps=1, resume=True)
+        assert r["status"] == 0
+        ents.append(r["tot_ent"])
+        u = o.u_con[:, :, :, 1:-1, 1:-1]
+        g = prob.gamma
+        rho = u[0]
+        p = (g - 1) * (u[7] - 0.5 * ((u[1] ** 2 + u[2] ** 2 + u[3] ** 2) / rho + (u[4] ** 2 + u[5] ** 2 + u[6] ** 2)))
+        assert rho.min() > 0 and p.min() > 0
+    # the total entropy of an outflow domain can rise only through the boundary; the blast is far
+    # from the boundary here, so it must not increase
+    assert all(b <= a + 1e-10 * abs(a) for a, b in zip(ents, ents[1:]))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_vortex_is_steady_in_comoving_frame(pkg, ora, p):
+    norms = []
+    for n in (32, 64):
+        prob = pkg.problems.make("vortex", bulk=(0.0, 0.0))
+        u0 = prob.initial_state(n, n, p)
+        o = ora.OracleSolver(n, n, p, p, 3, *prob.domain, prob.gamma, prob.bc_kind)
+        u = np.asfortranarray(u0.copy())
+        o.apply_bc(u)
+        ut, _ = o.semidiscretize(u)
+        norms.append(np.abs(ut).max())
+    # the residual of the exact steady state converges at about order p in the max norm
+    assert np.log2(norms[0] / norms[1]) >= p - 0.5, norms
+
+
+def test_vortex_exact_at_zero(pkg):
+    prob = pkg.problems.make("vortex")
+    u0 = prob.initial_state(8, 8, 2)[:, :, :, 1:-1, 1:-1]
+    np.testing.assert_allclose(pkg.problems.vortex_exact(8, 8, 2, 0.0), u0, rtol=0, atol=1e-14)
+    # one period: the exact solution returns to the initial state
+    np.testing.assert_allclose(pkg.problems.vortex_exact(8, 8, 2, 20.0), u0, rtol=0, atol=1e-12)
+
+
+def test_retry_path(pkg, ora):
+    prob, u0, o = make(pkg, ora, "blast", 16, 2)
+    r = o.solve(prob.final_T, 10.0, max_steps=4)
+    assert r["status"] == 0
+    assert r["retries"] > 0 and r["steps"] == 4
+    assert o.u_con[0, :, :, 1:-1, 1:-1].min() > 0
+
+
+def test_final_time_is_reached(pkg, ora):
+    prob, u0, o = make(pkg, ora, "ot2pi", 8, 1)
+    r = o.solve(0.05, prob.cfl)
+    assert r["status"] == 0
+    assert abs(r["t"] - 0.05) <= 1e-15
+
+
+def test_initial_inadmissible_average_is_reported(pkg, ora):
+    prob, u0, o = make(pkg, ora, "ot2pi", 6, 2)
+    u = o.u_con
+    u[7, :, :, 3, 3] = -1.0  # negative energy -> negative pressure average
+    r = o.solve(prob.final_T, prob.cfl, max_steps=1)
+    assert r["status"] == 2
