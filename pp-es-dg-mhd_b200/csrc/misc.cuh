@@ -251,8 +251,13 @@ __global__ void ctl_stage_end(Ctrl* c) {
   c->pending_dtlim = 1;
 }
 
-// end of a try: accept (drive.f90:304-312) or prepare the re-try
+// end of a try: accept (drive.f90:304-312) or prepare the re-try.  dt_lim is the value of the
+// last residual that ran, as in the reference, where every DG_semidiscretize overwrites it.
 __global__ void ctl_step_end(Ctrl* c, int R) {
+  if (c->pending_dtlim) {
+    c->dt_lim = dec_dtlim(c->dt_lim_bits);
+    c->pending_dtlim = 0;
+  }
   if (c->state == ST_FAILED) {  // re-try with a smaller dt
     c->state = ST_IDLE;
     return;
