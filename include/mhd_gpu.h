@@ -163,6 +163,32 @@ int mhd_gpu_get_status(mhd_gpu_t *h, mhd_gpu_status *st);
  * keep data on the GPU, e.g. a PyTorch tensor view).  No reference counterpart. */
 int mhd_gpu_state_device_ptr(mhd_gpu_t *h, int slot, double **dptr);
 
+/* ---- allocation-free residual ------------------------------------------------------------ */
+
+/* No counterpart in the reference: an extra entry point of this library.
+ *
+ * ut = L(u) and dt_lim, the same computation as mhd_gpu_semidiscretize, for callers that must
+ * not allocate device memory: hosts whose device-memory budget is fully reserved up front by
+ * their own pool or memory manager, hosts running on a device whose allocations are capped by an
+ * external manager, and time-critical loops that cannot afford the implicit device-wide
+ * synchronisation a cudaMalloc/cudaFree may cause.  The caller owns and passes both arrays:
+ *   u   device pointer, state in the library's element-blocked layout with the ghost ring filled
+ *       ([ny+2][nx+2][8][(p+1)^2] doubles, the layout mhd_gpu_state_device_ptr exposes);
+ *   ut  device pointer, [ny][nx][8][(p+1)^2] doubles, written;
+ *   dt_lim  host pointer (may be NULL); when given, the call waits for the stream.
+ * The call allocates nothing: its only scratch (the dt_lim reduction cell and status words) is a
+ * 4 KiB static device array inside the library, which every GPU that loads the library holds
+ * until the process exits.  All calls share that array and it keeps the last call's contents;
+ * the reduction cell is reset at the start of every call, and calls that overlap on the GPU
+ * (different streams or host threads at the same time) race on it.
+ * The first call on a device sets that device up (constant tables, kernel attributes and the
+ * address of the static array); make that first call before any stream capture.
+ * Limits: px = py = p in 1..3, 2 <= nx, ny <= 4096; anything larger or any other argument out of
+ * range is rejected with MHD_ERR_UNSUPPORTED / MHD_ERR_INVALID before touching the GPU.
+ * stream: a cudaStream_t (NULL = the legacy default stream). */
+int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, double hy, double gamma,
+                                   const double *u, double *ut, double *dt_lim, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

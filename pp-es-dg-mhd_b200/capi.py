@@ -64,6 +64,8 @@ SIGNATURES = {
     "mhd_gpu_advance": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(Status)]),
     "mhd_gpu_get_status": (C.c_int, [_vp, C.POINTER(Status)]),
     "mhd_gpu_state_device_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_dp)]),
+    "mhd_gpu_semidiscretize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                                 C.c_double, _vp, _vp, _dp, _vp]),
 }
 
 _lib = None

@@ -612,3 +612,86 @@ int mhd_gpu_state_device_ptr(mhd_gpu_t* h, int slot, double** dptr) {
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free residual.  Its only scratch (the dt_lim reduction cell and the status words of
+// the control block that residual_kernel writes) lives in this file-scope static device array;
+// host code reaches it through the address cudaGetSymbolAddress returns for the current device.
+// =============================================================================================
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 4096;
+static_assert(sizeof(Ctrl) <= kNoAllocScratchBytes, "control block must fit the static scratch");
+constexpr int kNoAllocMaxCells = 4096;  // per direction
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
+
+// Once per device, with that device current: tables + kernel attributes, then the symbol address.
+int noalloc_setup(int dev, void** addr) {
+  int rc = init_device_tables(dev);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) return MHD_ERR_CUDA;
+    g_noalloc_addr[dev] = ptr;
+  }
+  *addr = g_noalloc_addr[dev];
+  return MHD_OK;
+}
+
+}  // namespace
+
+extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, double hy, double gamma,
+                                              const double* u, double* ut, double* dt_lim, void* stream) {
+  if (!u || !ut || !(hx > 0.0) || !(hy > 0.0) || !(gamma > 1.0) || nx < 2 || ny < 2) return MHD_ERR_INVALID;
+  if (p < 1 || p > MAXP || nx > kNoAllocMaxCells || ny > kNoAllocMaxCells) return MHD_ERR_UNSUPPORTED;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return MHD_ERR_INVALID;
+  void* addr = nullptr;
+  int rc = noalloc_setup(dev, &addr);
+  if (rc) return rc;
+  Ctrl* ctrl = static_cast<Ctrl*>(addr);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the reduction cell must start "empty" (all ones: above every positive double's bit pattern)
+  CK(cudaMemsetAsync(&ctrl->dt_lim_bits, 0xFF, sizeof(unsigned long long), s));
+  Geo g;
+  std::memset(&g, 0, sizeof(g));
+  g.nx = nx;
+  g.ny = ny;
+  g.hx = hx;
+  g.hy = hy;
+  g.gamma = gamma;
+  switch (p) {
+    case 1: {
+      using L = ResLayout<1>;
+      residual_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<1>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS);
+      break;
+    }
+    case 2: {
+      using L = ResLayout<2>;
+      residual_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<2>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS);
+      break;
+    }
+    default: {
+      using L = ResLayout<3>;
+      residual_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<3>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS);
+      break;
+    }
+  }
+  CK(cudaGetLastError());
+  if (dt_lim) {
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, &ctrl->dt_lim_bits, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double d;
+    std::memcpy(&d, &bits, sizeof(d));
+    *dt_lim = d;
+  }
+  return MHD_OK;
+}
