@@ -22,14 +22,30 @@
 #include <omp.h>
 #endif
 
+/* Extended precision for the one-time tables.  A counting build (oracle/flop_count.cpp) defines
+ * ORA_LDBL_DEFINED before replacing `double` by an operation-counting type. */
+#ifndef ORA_LDBL_DEFINED
+typedef long double ldbl;
+#endif
+/* hook for counting min/max as one operation each (empty in the normal builds) */
+#ifndef ORA_COUNT_MINMAX
+#define ORA_COUNT_MINMAX()
+#endif
+
 #define NQMAX 7          /* max nodes per direction (p<=6), gauss.f90:34-64 */
 #define NNMAX (NQMAX * NQMAX)
 
 static const double PP_eps = 1.0e-11;   /* DG_solver.f90:17 */
 static const double OEDG_eps = 1.0e-8;  /* DG_solver.f90:148 */
 
-static inline double dmax(double a, double b) { return a > b ? a : b; }
-static inline double dmin(double a, double b) { return a < b ? a : b; }
+static inline double dmax(double a, double b) {
+  ORA_COUNT_MINMAX();
+  return a > b ? a : b;
+}
+static inline double dmin(double a, double b) {
+  ORA_COUNT_MINMAX();
+  return a < b ? a : b;
+}
 static inline int imax(int a, int b) { return a > b ? a : b; }
 
 /* _macro_prs_ (DG_solver.f90:125) */
@@ -47,7 +63,7 @@ static inline double ent_macro(double rho, double prs, double gamma) {
 /* matrices are computed from their definitions in extended precision and rounded once.        */
 /* ------------------------------------------------------------------------------------------ */
 
-static void legendre_all(int N, long double x, long double *P, long double *dP) {
+static void legendre_all(int N, ldbl x, ldbl *P, ldbl *dP) {
   /* P[k] = P_k(x), dP[k] = P_k'(x), k=0..N (recurrence as gauss.f90:390-434 states it) */
   P[0] = 1.0L;
   dP[0] = 0.0L;
@@ -61,9 +77,9 @@ static void legendre_all(int N, long double x, long double *P, long double *dP) 
   }
 }
 
-static int invert_ld(int n, const long double *A, long double *Ainv) {
+static int invert_ld(int n, const ldbl *A, ldbl *Ainv) {
   /* Gauss-Jordan with partial pivoting, column-major n x n */
-  long double W[NQMAX][2 * NQMAX];
+  ldbl W[NQMAX][2 * NQMAX];
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < n; ++j) {
       W[i][j] = A[i + n * j];
@@ -76,15 +92,15 @@ static int invert_ld(int n, const long double *A, long double *Ainv) {
     if (W[piv][c] == 0.0L) return -1;
     if (piv != c)
       for (int j = 0; j < 2 * n; ++j) {
-        long double t = W[c][j];
+        ldbl t = W[c][j];
         W[c][j] = W[piv][j];
         W[piv][j] = t;
       }
-    long double d = W[c][c];
+    ldbl d = W[c][c];
     for (int j = 0; j < 2 * n; ++j) W[c][j] /= d;
     for (int r = 0; r < n; ++r)
       if (r != c) {
-        long double f = W[r][c];
+        ldbl f = W[r][c];
         if (f != 0.0L)
           for (int j = 0; j < 2 * n; ++j) W[r][j] -= f * W[c][j];
       }
@@ -95,33 +111,33 @@ static int invert_ld(int n, const long double *A, long double *Ainv) {
 }
 
 /* GLL nodes/weights (gauss.f90:17-71) and nodal matrices (gauss.f90:134-331), extended precision */
-static int gll_tables_ld(int p, long double *x, long double *w, long double *M, long double *Minv,
-                         long double *D, long double *Pmn, long double *Pnm) {
+static int gll_tables_ld(int p, ldbl *x, ldbl *w, ldbl *M, ldbl *Minv,
+                         ldbl *D, ldbl *Pmn, ldbl *Pnm) {
   const int n = p + 1, N = p;
   if (p < 0 || p > 6) return -1;
-  long double P[NQMAX + 1], dP[NQMAX + 1];
+  ldbl P[NQMAX + 1], dP[NQMAX + 1];
   if (p == 0) {
     x[0] = 0.0L;
     w[0] = 2.0L;
   } else {
     x[0] = -1.0L;
     x[N] = 1.0L;
-    const long double pi = 3.141592653589793238462643383279502884L;
+    const ldbl pi = 3.141592653589793238462643383279502884L;
     for (int i = 1; i < N; ++i) {
-      long double xi = -cosl(pi * i / N);
+      ldbl xi = -cosl(pi * i / N);
       for (int it = 0; it < 200; ++it) {
         legendre_all(N, xi, P, dP);
         /* f = P_N'(x), f' = P_N''(x) from the Legendre equation */
-        long double f = dP[N];
-        long double fp = (2.0L * xi * dP[N] - N * (N + 1) * P[N]) / (1.0L - xi * xi);
-        long double dx = f / fp;
+        ldbl f = dP[N];
+        ldbl fp = (2.0L * xi * dP[N] - N * (N + 1) * P[N]) / (1.0L - xi * xi);
+        ldbl dx = f / fp;
         xi -= dx;
         if (fabsl(dx) < 1e-30L) break;
       }
       x[i] = xi;
     }
     for (int i = 0; i < n / 2; ++i) { /* exact symmetry of the node set */
-      long double a = 0.5L * (x[N - i] - x[i]);
+      ldbl a = 0.5L * (x[N - i] - x[i]);
       x[i] = -a;
       x[N - i] = a;
     }
@@ -140,7 +156,7 @@ static int gll_tables_ld(int p, long double *x, long double *w, long double *M, 
   /* exact mass matrix of the Lagrange basis: M = Pnm^T diag(2/(2m+1)) Pnm */
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < n; ++j) {
-      long double acc = 0.0L;
+      ldbl acc = 0.0L;
       for (int m = 0; m < n; ++m) acc += Pnm[m + n * i] * Pnm[m + n * j] * (2.0L / (2 * m + 1));
       M[i + n * j] = acc;
     }
@@ -149,7 +165,7 @@ static int gll_tables_ld(int p, long double *x, long double *w, long double *M, 
   if (p == 0) {
     D[0] = 0.0L;
   } else {
-    long double PN[NQMAX];
+    ldbl PN[NQMAX];
     for (int i = 0; i < n; ++i) {
       legendre_all(N, x[i], P, dP);
       PN[i] = P[N];
@@ -159,9 +175,9 @@ static int gll_tables_ld(int p, long double *x, long double *w, long double *M, 
         if (i != j)
           D[i + n * j] = PN[i] / (PN[j] * (x[i] - x[j]));
         else if (i == 0)
-          D[i + n * j] = -(long double)(N * (N + 1)) / 4.0L;
+          D[i + n * j] = -(ldbl)(N * (N + 1)) / 4.0L;
         else if (i == N)
-          D[i + n * j] = (long double)(N * (N + 1)) / 4.0L;
+          D[i + n * j] = (ldbl)(N * (N + 1)) / 4.0L;
         else
           D[i + n * j] = 0.0L;
       }
@@ -171,7 +187,7 @@ static int gll_tables_ld(int p, long double *x, long double *w, long double *M, 
 
 int ora_gll_tables(int p, double *x, double *w, double *M, double *Minv, double *D, double *Pmn,
                    double *Pnm) {
-  long double lx[NQMAX], lw[NQMAX], lM[NNMAX], lMi[NNMAX], lD[NNMAX], lPmn[NNMAX], lPnm[NNMAX];
+  ldbl lx[NQMAX], lw[NQMAX], lM[NNMAX], lMi[NNMAX], lD[NNMAX], lPmn[NNMAX], lPnm[NNMAX];
   int rc = gll_tables_ld(p, lx, lw, lM, lMi, lD, lPmn, lPnm);
   if (rc) return rc;
   int n = p + 1;
@@ -225,7 +241,7 @@ typedef struct {
  * of G are the accumulated rotations V.  The projector built from (U, L) is invariant to the
  * sign and in-eigenspace basis freedom of U. */
 static void svd_left(int n, const double *G, double *U, double *L) {
-  long double A[NQMAX][NQMAX], V[NQMAX][NQMAX]; /* A[c][r]: column c of G^T = row c of G */
+  ldbl A[NQMAX][NQMAX], V[NQMAX][NQMAX]; /* A[c][r]: column c of G^T = row c of G */
   for (int c = 0; c < n; ++c)
     for (int r = 0; r < n; ++r) {
       A[c][r] = G[c + n * r]; /* (G^T)(r,c) = G(c,r) */
@@ -235,7 +251,7 @@ static void svd_left(int n, const double *G, double *U, double *L) {
     int rotated = 0;
     for (int p = 0; p < n - 1; ++p)
       for (int q = p + 1; q < n; ++q) {
-        long double al = 0, be = 0, ga = 0;
+        ldbl al = 0, be = 0, ga = 0;
         for (int r = 0; r < n; ++r) {
           al += A[p][r] * A[p][r];
           be += A[q][r] * A[q][r];
@@ -243,24 +259,24 @@ static void svd_left(int n, const double *G, double *U, double *L) {
         }
         if (ga == 0.0L || fabsl(ga) <= 1e-30L * sqrtl(al * be)) continue;
         rotated = 1;
-        long double zeta = (be - al) / (2.0L * ga);
-        long double t = (zeta >= 0 ? 1.0L : -1.0L) / (fabsl(zeta) + sqrtl(1.0L + zeta * zeta));
-        long double c = 1.0L / sqrtl(1.0L + t * t), s = c * t;
+        ldbl zeta = (be - al) / (2.0L * ga);
+        ldbl t = (zeta >= 0 ? 1.0L : -1.0L) / (fabsl(zeta) + sqrtl(1.0L + zeta * zeta));
+        ldbl c = 1.0L / sqrtl(1.0L + t * t), s = c * t;
         for (int r = 0; r < n; ++r) {
-          long double ap = A[p][r], aq = A[q][r];
+          ldbl ap = A[p][r], aq = A[q][r];
           A[p][r] = c * ap - s * aq;
           A[q][r] = s * ap + c * aq;
-          long double vp = V[p][r], vq = V[q][r];
+          ldbl vp = V[p][r], vq = V[q][r];
           V[p][r] = c * vp - s * vq;
           V[q][r] = s * vp + c * vq;
         }
       }
     if (!rotated) break;
   }
-  long double sv[NQMAX];
+  ldbl sv[NQMAX];
   int order[NQMAX];
   for (int c = 0; c < n; ++c) {
-    long double acc = 0;
+    ldbl acc = 0;
     for (int r = 0; r < n; ++r) acc += A[c][r] * A[c][r];
     sv[c] = sqrtl(acc);
     order[c] = c;
@@ -640,7 +656,12 @@ ora_solver *ora_create(int nx, int ny, int px, int py, int rknstg, double left, 
   s->top = top;
   s->gamma = gamma;
   s->bc_kind = bc_kind;
-  for (int v = 0; v < 8; ++v) s->bc_state[v] = bc_state8 ? bc_state8[v] : NAN;
+  for (int v = 0; v < 8; ++v) {
+    if (bc_state8)
+      s->bc_state[v] = bc_state8[v];
+    else
+      s->bc_state[v] = NAN;
+  }
   ora_gll_tables(px, s->qx_x, s->qw_x, s->M_x, s->Minv_x, s->diff_x, s->Pmn_x, s->Pnm_x);
   ora_gll_tables(py, s->qx_y, s->qw_y, s->M_y, s->Minv_y, s->diff_y, s->Pmn_y, s->Pnm_y);
   ldf_init(&s->ldf, px, py);
@@ -1414,6 +1435,7 @@ int ora_solve_resume(ora_solver *s, double final_T, double cfl, int use_oedg, in
   int neg_avg = 0, num_negcell = 0, relimit = 0;
   long total_negcell = 0;
   int steps = 0, retries = 0, status = ORA_OK;
+  int flag = 1;
   if (resume) {
     t = s->run_t;
     dt = s->run_dt;
@@ -1431,7 +1453,7 @@ int ora_solve_resume(ora_solver *s, double final_T, double cfl, int use_oedg, in
   ora_apply_bc(s, s->u_con);
   ora_semidiscretize(s, ora_ut_con(s, 1), &dt_lim, s->u_con);
 loop:;
-  int flag = 1;
+  flag = 1;
   while (flag) {
     if (max_steps > 0 && steps >= max_steps) break;
     steps++;

@@ -18,14 +18,15 @@
 
 namespace mhd {
 
+// Tile (TX x TY elements), threads per CTA and the CTAs per SM the register budget is cut for.
 template <int P>
 struct ResCfg;
 template <>
-struct ResCfg<1> { static constexpr int TX = 8, TY = 8, NT = 256; };
+struct ResCfg<1> { static constexpr int TX = 8, TY = 4, NT = 128, MINB = 4; };
 template <>
-struct ResCfg<2> { static constexpr int TX = 4, TY = 4, NT = 256; };
+struct ResCfg<2> { static constexpr int TX = 4, TY = 4, NT = 128, MINB = 4; };
 template <>
-struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 256; };
+struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 128, MINB = 4; };
 
 template <int P>
 struct ResLayout {
@@ -36,7 +37,12 @@ struct ResLayout {
   static constexpr int NPAIR = 2 * NPX;
   static constexpr int NFX = (TX + 1) * TY * N;
   static constexpr int NFY = TX * (TY + 1) * N;
-  static constexpr int FW = 11;  // face record: flux[8], nB, sl, sr
+  static constexpr int FW = 11;  // face record: flux[8], nB, sl, sr (stored component-major)
+  // threads of phase 2 given to the face nodes: a whole number of warps, cost-proportional
+  static constexpr int NT_ = ResCfg<P>::NT;
+  static constexpr int THL_RAW = (NT_ * (NFX + NFY) * 9) / ((NFX + NFY) * 9 + TE * NPAIR * 5);
+  static constexpr int THL_W = (THL_RAW + 16) / 32 * 32;
+  static constexpr int THL = THL_W < 32 ? 32 : (THL_W > NT_ - 32 ? NT_ - 32 : THL_W);
   // offsets in doubles
   static constexpr int O_CONS = 0;
   static constexpr int O_PRIM = O_CONS + TE * EB;
@@ -65,7 +71,7 @@ __device__ __forceinline__ void pair_ab(int idx, int& a, int& b) {
 __device__ __forceinline__ int pair_index(int a, int b) { return a * (a - 1) / 2 + b; }
 
 template <int P>
-__global__ void __launch_bounds__(ResCfg<P>::NT, 1)
+__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
     residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl,
                     int gate) {
   using L = ResLayout<P>;
@@ -150,9 +156,16 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
   __syncthreads();
 
   // ---- phase 2: interface fluxes and element pair fluxes ----
+  // Warp-specialised: the first THL threads (whole warps) take the face nodes, the others the
+  // node pairs, split in proportion to their cost (one HLL flux ~ 1.8 EC fluxes).
   {
-    constexpr int NITEM = L::NFX + L::NFY + TE * L::NPAIR;
-    for (int it = tid; it < NITEM; it += NT) {
+    constexpr int NH = L::NFX + L::NFY, NPT = TE * L::NPAIR;
+    constexpr int THL = L::THL;
+    const bool hll_thread = tid < THL;
+    const int first = hll_thread ? tid : NH + (tid - THL);
+    const int stride = hll_thread ? THL : NT - THL;
+    const int last = hll_thread ? NH : NH + NPT;
+    for (int it = first; it < last; it += stride) {
       if (it < L::NFX) {  // x face node
         const int fi = it / (TY * N), rem = it - fi * TY * N, r = rem / N, l = rem - r * N;
         if (r >= H || fi > W) continue;
@@ -162,7 +175,10 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
           wl[v] = (fi == 0) ? s_hxl[(r * 8 + v) * N + l] : s_cons[(r * TX + fi - 1) * EB + v * NN + (N - 1) + N * l];
           wr[v] = (fi == W) ? s_hxr[(r * 8 + v) * N + l] : s_cons[(r * TX + fi) * EB + v * NN + N * l];
         }
-        espp_hll(wl, wr, gamma, s_fx + it * L::FW);
+        double o[11];
+        espp_hll(wl, wr, gamma, o);
+#pragma unroll
+        for (int c = 0; c < L::FW; ++c) s_fx[c * L::NFX + it] = o[c];  // component-major: no bank conflicts
       } else if (it < L::NFX + L::NFY) {  // y face node (swap_xy in and out)
         const int f = it - L::NFX;
         const int fj = f / (TX * N), rem = f - fj * TX * N, c = rem / N, k = rem - c * N;
@@ -177,18 +193,18 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
         double sb[8] = {b[0], b[2], b[1], b[3], b[5], b[4], b[6], b[7]};
         double o[11];
         espp_hll(sa, sb, gamma, o);
-        double* dst = s_fy + f * L::FW;
-        dst[0] = o[0];
-        dst[1] = o[2];
-        dst[2] = o[1];
-        dst[3] = o[3];
-        dst[4] = o[5];
-        dst[5] = o[4];
-        dst[6] = o[6];
-        dst[7] = o[7];
-        dst[8] = o[8];
-        dst[9] = o[9];
-        dst[10] = o[10];
+        double* dst = s_fy + f;
+        dst[0 * L::NFY] = o[0];
+        dst[1 * L::NFY] = o[2];
+        dst[2 * L::NFY] = o[1];
+        dst[3 * L::NFY] = o[3];
+        dst[4 * L::NFY] = o[5];
+        dst[5 * L::NFY] = o[4];
+        dst[6 * L::NFY] = o[6];
+        dst[7 * L::NFY] = o[7];
+        dst[8 * L::NFY] = o[8];
+        dst[9 * L::NFY] = o[9];
+        dst[10 * L::NFY] = o[10];
       } else {  // element node pair
         const int pidx = it - L::NFX - L::NFY;
         const int e = pidx / L::NPAIR, pi = pidx - e * L::NPAIR;
@@ -218,9 +234,9 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
           }
           ec_flux<1>(A, B, gamma, F);
         }
-        double* dst = s_pair + (e * L::NPAIR + pi) * 8;
+        double* dst = s_pair + e * L::NPAIR + pi;  // variable-major: no bank conflicts
 #pragma unroll
-        for (int v = 0; v < 8; ++v) dst[v] = F[v];
+        for (int v = 0; v < 8; ++v) dst[v * TE * L::NPAIR] = F[v];
       }
     }
   }
@@ -289,14 +305,15 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
 #pragma unroll
       for (int v = 0; v < 8; ++v) acc[v] = -(ckk * F[v]) - cll * G[v] - divB * GP[v];
       // pair contributions along x (line l) and y (column k)
-      const double* pe = s_pair + e * L::NPAIR * 8;
+      const double* pe = s_pair + e * L::NPAIR;
+      constexpr int PS = TE * L::NPAIR;  // stride between variables
 #pragma unroll
       for (int r = 0; r < N; ++r) {
         if (r == k) continue;
         const int pi = l * L::NPR + pair_index(max(k, r), min(k, r));
         const double c = 2.0 * sxh * dc.D[k + N * r];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[pi * 8 + v];
+        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
       }
 #pragma unroll
       for (int m = 0; m < N; ++m) {
@@ -304,32 +321,32 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
         const int pi = L::NPX + k * L::NPR + pair_index(max(l, m), min(l, m));
         const double c = 2.0 * syh * dc.D[l + N * m];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[pi * 8 + v];
+        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
       }
       // surface terms (DG_solver.f90:872-882)
       if (k == 0) {
-        const double* fr = s_fx + ((ec * TY + er) * N + l) * L::FW;
+        const double* fr = s_fx + ((ec * TY + er) * N + l);
         const double c = sxh / dc.qw[0];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * (F[v] - fr[v] + GP[v] * (bx - fr[8]));
+        for (int v = 0; v < 8; ++v) acc[v] -= c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
       }
       if (k == N - 1) {
-        const double* fr = s_fx + (((ec + 1) * TY + er) * N + l) * L::FW;
+        const double* fr = s_fx + (((ec + 1) * TY + er) * N + l);
         const double c = sxh / dc.qw[N - 1];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v] + GP[v] * (bx - fr[8]));
+        for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
       }
       if (l == 0) {
-        const double* fr = s_fy + ((er * TX + ec) * N + k) * L::FW;
+        const double* fr = s_fy + ((er * TX + ec) * N + k);
         const double c = syh / dc.qw[0];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * (G[v] - fr[v] + GP[v] * (by - fr[8]));
+        for (int v = 0; v < 8; ++v) acc[v] -= c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
       }
       if (l == N - 1) {
-        const double* fr = s_fy + (((er + 1) * TX + ec) * N + k) * L::FW;
+        const double* fr = s_fy + (((er + 1) * TX + ec) * N + k);
         const double c = syh / dc.qw[N - 1];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v] + GP[v] * (by - fr[8]));
+        for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
       }
 #pragma unroll
       for (int v = 0; v < 8; ++v) cw[v * NN] = acc[v];  // own node only: safe in place
@@ -344,12 +361,12 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, 1)
       }
       double mxr = -1.0e300, mnl = 1.0e300, myu = -1.0e300, mnd = 1.0e300;
       for (int l = 0; l < N; ++l) {
-        mxr = fmax(mxr, s_fx[((ec * TY + er) * N + l) * L::FW + 10]);
-        mnl = fmin(mnl, s_fx[(((ec + 1) * TY + er) * N + l) * L::FW + 9]);
+        mxr = fmax(mxr, s_fx[10 * L::NFX + (ec * TY + er) * N + l]);
+        mnl = fmin(mnl, s_fx[9 * L::NFX + ((ec + 1) * TY + er) * N + l]);
       }
       for (int k = 0; k < N; ++k) {
-        myu = fmax(myu, s_fy[((er * TX + ec) * N + k) * L::FW + 10]);
-        mnd = fmin(mnd, s_fy[(((er + 1) * TX + ec) * N + k) * L::FW + 9]);
+        myu = fmax(myu, s_fy[10 * L::NFY + (er * TX + ec) * N + k]);
+        mnd = fmin(mnd, s_fy[9 * L::NFY + ((er + 1) * TX + ec) * N + k]);
       }
       const double ax = fmax(fmax(sx, mxr), -mnl), ay = fmax(fmax(sy, myu), -mnd);
       const double dtl = 1.0 / ((2 * P + 1) * ax / g.hx + (2 * P + 1) * ay / g.hy);

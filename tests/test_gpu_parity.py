@@ -17,6 +17,16 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+def _ent_tol(u, gamma):
+    """tolerance for the total entropy: 1e-13 relative times the conditioning of the pressure,
+    max(E/p) over the nodes (p = (gamma-1)(E - kinetic - magnetic) loses that factor of relative
+    accuracy, and the entropy depends on log p); ~4000 for the low-beta blast"""
+    x = u[:, :, :, 1:-1, 1:-1]
+    prs = (gamma - 1) * (x[7] - 0.5 * ((x[1] ** 2 + x[2] ** 2 + x[3] ** 2) / x[0] + (x[4] ** 2 + x[5] ** 2 + x[6] ** 2)))
+    cond = np.max(np.abs(x[7]) / np.maximum(np.abs(prs), 1e-300))
+    return 1e-13 * max(1.0, float(cond))
+
+
 def _setup(pkg, ora, name, nx, ny, p, amp=1.0, rknstg=3):
     prob = pkg.problems.make(name, amp=amp)
     u0 = prob.initial_state(nx, ny, p)
@@ -91,7 +101,7 @@ def test_post_process_parity(pkg, ora, name, nx, ny, p, oedg, ldf, comput_ent, e
     assert not ro["neg_avg"], "case must stay admissible"
     assert rg["num_negcell"] == ro["num_negcell"]
     if comput_ent and not ro["neg_avg"]:
-        assert abs(rg["tot_ent"] - ro["tot_ent"]) <= 1e-13 * abs(ro["tot_ent"])
+        assert abs(rg["tot_ent"] - ro["tot_ent"]) <= _ent_tol(uo, prob.gamma) * abs(ro["tot_ent"])
     else:
         assert np.isnan(rg["tot_ent"]) and np.isnan(ro["tot_ent"])
     ug = g.download_state(0)
@@ -128,7 +138,7 @@ def test_pp_limiter_parity(pkg, ora, oedg):
     assert not ro["neg_avg"] and not rg["neg_avg"]
     assert ro["num_negcell"] >= 1
     assert rg["num_negcell"] == ro["num_negcell"]
-    assert abs(rg["tot_ent"] - ro["tot_ent"]) <= 1e-13 * abs(ro["tot_ent"])
+    assert abs(rg["tot_ent"] - ro["tot_ent"]) <= _ent_tol(uo, prob.gamma) * abs(ro["tot_ent"])
     ug = g.download_state(0)
     m = np.isfinite(uo)
     err = rel_l1(np.where(m, ug, 0.0), np.where(m, uo, 0.0))
