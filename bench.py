@@ -224,6 +224,56 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------------------ serving leg
+HORIZON = {"ot2pi": 0.5, "rotor": 0.15, "blast": 0.01}
+
+
+def make_requests(n_req, rate, seed, n_lo, n_hi, t_scale):
+    """seeded request stream: Poisson arrivals at `rate`/s; problem in {OT, rotor, blast}; mesh N^2
+    with N log-uniform in [n_lo, n_hi]; degree uniform in {1,2,3}; t_end uniform in [0.05, 0.5] x
+    the problem's horizon (x t_scale)"""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for i in range(n_req):
+        t += rng.exponential(1.0 / rate)
+        name = ["ot2pi", "rotor", "blast"][int(rng.integers(0, 3))]
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        p = int(rng.integers(1, 4))
+        t_end = float(rng.uniform(0.05, 0.5)) * HORIZON[name] * t_scale
+        reqs.append(dict(id=i, name=name, n=n, p=p, t_end=t_end, arrival=t))
+    return reqs
+
+
+def serve(pkg, reqs, batched, budget, tries_per_round=2):
+    srv = pkg.Server(budget, max_active=4096, tries_per_round=tries_per_round, batched=batched)
+    for r in reqs:
+        prob = pkg.problems.make(r["name"])
+        srv.submit(r["id"], prob, r["n"], r["n"], r["p"], r["u0"], r["arrival"], final_T=r["t_end"])
+    t0 = time.perf_counter()
+    srv.run()
+    wall = time.perf_counter() - t0
+    res = srv.results()
+    srv.close()
+    tts = np.array([x["finished"] - x["arrival"] for x in res])
+    makespan = max(x["finished"] for x in res) - min(x["arrival"] for x in res)
+    ok = sum(1 for x in res if x["done"] == 1 and x["flags"] == 0 and x["error"] == 0)
+    return {"solves_per_s": len(res) / makespan, "p50_tts_s": float(np.percentile(tts, 50)),
+            "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok, "requests": len(reqs),
+            "wall_s": wall, "steps": int(sum(x["steps"] for x in res))}
+
+
+def serve_leg(pkg, n_req=48, rate=400.0, seed=7, n_lo=32, n_hi=192, t_scale=0.2, budget=64 << 30):
+    reqs = make_requests(n_req, rate, seed, n_lo, n_hi, t_scale)
+    for r in reqs:
+        r["u0"] = pkg.problems.make(r["name"]).initial_state(r["n"], r["n"], r["p"])
+    b = serve(pkg, reqs, True, budget)
+    q = serve(pkg, reqs, False, budget)
+    return {"batched": b, "one_at_a_time": q, "speedup_solves_per_s": b["solves_per_s"] / q["solves_per_s"],
+            "stream": f"{n_req} requests, Poisson {rate:g}/s, seed {seed}, N log-uniform [{n_lo},{n_hi}], "
+                      f"p in 1..3, problem in {{OT, rotor, blast}}, t_end U[0.05,0.5] x horizon x {t_scale:g}"}
+
+
 # ------------------------------------------------------------------------------ GPU leg
 def run_ours(args):
     import torch
@@ -349,6 +399,8 @@ def run_ours(args):
         }
         if e2e:
             line["e2e"] = e2e
+        if not args.no_serve and ws == 1:
+            line["served"] = serve_leg(pkg)
         if not args.no_cpu and ws == 1:
             line["cpu_baseline"] = cpu_sample(prob_name, n, p, oedg, ldf, budget_s=args.cpu_budget)
         print(json.dumps(line), flush=True)
@@ -368,6 +420,7 @@ def main():
     ap.add_argument("--workload", default="vortex512_p3", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -163,6 +163,72 @@ int mhd_gpu_get_status(mhd_gpu_t *h, mhd_gpu_status *st);
  * keep data on the GPU, e.g. a PyTorch tensor view).  No reference counterpart. */
 int mhd_gpu_state_device_ptr(mhd_gpu_t *h, int slot, double **dptr);
 
+/* ---- batches of independent instances ---------------------------------------------------- */
+
+/* No reference counterpart (the reference runs one instance per process).  A batch advances many
+ * independent solver instances together: one CUDA graph per SSP-RK try runs the batched kernels
+ * (persistent grids over a flattened work list of every member's tiles), grouped by (p, rknstg).
+ * Each member computes exactly what mhd_gpu_advance would compute for it alone.
+ * Members must be on the batch's device and past mhd_gpu_solve_begin; while in a batch a member is
+ * driven only by the batch (its status is still readable); remove it before destroying it. */
+typedef struct mhd_batch mhd_batch_t;
+int mhd_batch_create(mhd_batch_t **out);
+int mhd_batch_destroy(mhd_batch_t *b);
+int mhd_batch_add(mhd_batch_t *b, mhd_gpu_t *h);
+int mhd_batch_remove(mhd_batch_t *b, mhd_gpu_t *h);
+int mhd_batch_size(const mhd_batch_t *b, int *n);
+/* `tries` graph launches (each member takes one try of a time step per launch: an accepted step,
+ * a re-try, or nothing once done), then a refresh of every member's status; *n_active (may be
+ * NULL) = members neither done nor failed. */
+int mhd_batch_advance(mhd_batch_t *b, int tries, int *n_active);
+/* a member's status as of the last mhd_batch_advance */
+int mhd_batch_member_status(mhd_batch_t *b, mhd_gpu_t *h, mhd_gpu_status *st);
+
+/* ---- serving ------------------------------------------------------------------------------ */
+
+/* No reference counterpart.  Device bytes mhd_gpu_create would allocate for one instance (the
+ * admission price of a run). */
+int mhd_gpu_footprint(int nx, int ny, int p, int rknstg, size_t *bytes);
+
+/* One run = one solve_execute: configuration, initial state and an arrival time (seconds on the
+ * server clock, which starts at the first mhd_server_run). */
+typedef struct mhd_request {
+  long long id;
+  int nx, ny, p, rknstg;
+  double left, right, bottom, top, gamma;
+  int bc_kind;
+  int pad_;
+  double bc_state8[8];
+  double final_T, cfl;
+  int use_oedg, use_ldf, ent_offset;
+  int pad2_;
+  double arrival;
+  const double *u0;   /* host, Fortran layout u(8,p+1,p+1,0:nx+1,0:ny+1); valid until finished */
+  double *u_avg_out;  /* host, receives u_avg (8,0:nx+1,0:ny+1) at the end; may be NULL */
+} mhd_request;
+
+typedef struct mhd_request_result {
+  long long id;
+  double arrival, admitted, finished;  /* server clock, seconds */
+  double t;                            /* simulated time reached */
+  long long steps, retries;
+  int done, flags, error, pad_;
+} mhd_request_result;
+
+/* A request loop with continuous batching: runs are admitted when they have arrived and their
+ * footprint fits the HBM budget (at most max_active at once), all active runs advance together in
+ * one batch (tries_per_round batched tries between polls), finished runs retire and free their
+ * memory.  batched = 0 serves the same queue one plain run at a time (the comparison point). */
+typedef struct mhd_server mhd_server_t;
+int mhd_server_create(size_t hbm_budget_bytes, int max_active, int tries_per_round, int batched,
+                      mhd_server_t **out);
+int mhd_server_submit(mhd_server_t *s, const mhd_request *r);
+/* serve until every submitted run has finished, or max_seconds (<= 0: no limit) of wall time */
+int mhd_server_run(mhd_server_t *s, double max_seconds);
+int mhd_server_pending(const mhd_server_t *s, int *queued, int *active, size_t *used_bytes);
+int mhd_server_results(const mhd_server_t *s, mhd_request_result *out, int cap, int *n);
+int mhd_server_destroy(mhd_server_t *s);
+
 /* ---- allocation-free residual ------------------------------------------------------------ */
 
 /* No counterpart in the reference: an extra entry point of this library.

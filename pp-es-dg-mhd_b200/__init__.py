@@ -27,7 +27,7 @@ import numpy as np
 from . import capi, problems
 from .capi import (BC_EXTRAPOLATE, BC_FIXED, BC_PERIODIC, BC_XEXTRAP_YPER, MHDError, Status)
 
-__all__ = ["DGSolver", "MHDError", "capi", "problems", "BC_PERIODIC", "BC_EXTRAPOLATE",
+__all__ = ["DGSolver", "Batch", "Server", "footprint", "MHDError", "capi", "problems", "BC_PERIODIC", "BC_EXTRAPOLATE",
            "BC_FIXED", "BC_XEXTRAP_YPER", "library_path", "ldf_operator"]
 
 _dp = C.POINTER(C.c_double)
@@ -213,3 +213,137 @@ class DGSolver:
         st = self.advance(max_steps)
         st["initial"] = info
         return st
+
+
+class Batch:
+    """Many independent solver instances advanced together (mhd_batch_*).
+
+    Members are DGSolver objects already through solve_begin.  Each member computes exactly what
+    it would compute alone; the batch only packs their work into shared launches."""
+
+    def __init__(self):
+        self.lib = capi.load()
+        h = C.c_void_p()
+        _check("mhd_batch_create", self.lib.mhd_batch_create(C.byref(h)))
+        self.h = h
+        self.members = []
+
+    def add(self, solver):
+        _check("mhd_batch_add", self.lib.mhd_batch_add(self.h, solver.h))
+        self.members.append(solver)
+
+    def remove(self, solver):
+        _check("mhd_batch_remove", self.lib.mhd_batch_remove(self.h, solver.h))
+        self.members.remove(solver)
+
+    def __len__(self):
+        n = C.c_int()
+        _check("mhd_batch_size", self.lib.mhd_batch_size(self.h, C.byref(n)))
+        return n.value
+
+    def advance(self, tries=1):
+        """`tries` batched tries; returns the number of members neither done nor failed"""
+        n = C.c_int()
+        _check("mhd_batch_advance", self.lib.mhd_batch_advance(self.h, int(tries), C.byref(n)))
+        return n.value
+
+    def status(self, solver):
+        st = Status()
+        rc = self.lib.mhd_batch_member_status(self.h, solver.h, C.byref(st))
+        _check("mhd_batch_member_status", rc, fatal_flags=False)
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_batch_destroy(self.h)
+            self.h = None
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def footprint(nx, ny, p, rknstg=3):
+    """device bytes one instance needs (host-only)"""
+    b = C.c_size_t()
+    _check("mhd_gpu_footprint", capi.load().mhd_gpu_footprint(nx, ny, p, rknstg, C.byref(b)))
+    return b.value
+
+
+class Server:
+    """Continuous-batching request loop (mhd_server_*): admits runs by HBM footprint, keeps them
+    resident, advances all active runs in one batch, retires finished runs."""
+
+    def __init__(self, hbm_budget_bytes, max_active=1024, tries_per_round=4, batched=True):
+        self.lib = capi.load()
+        h = C.c_void_p()
+        _check("mhd_server_create", self.lib.mhd_server_create(int(hbm_budget_bytes), int(max_active),
+                                                               int(tries_per_round), int(batched), C.byref(h)))
+        self.h = h
+        self._keep = []  # host buffers must outlive the runs
+
+    def submit(self, rid, prob, nx, ny, p, u0, arrival, final_T=None, rknstg=3, use_oedg=True,
+               use_ldf=True, ent_offset=False, want_avg=False):
+        u0 = np.asfortranarray(u0, dtype=np.float64)
+        r = capi.Request()
+        r.id = rid
+        r.nx, r.ny, r.p, r.rknstg = nx, ny, p, rknstg
+        r.left, r.right, r.bottom, r.top = map(float, prob.domain)
+        r.gamma = prob.gamma
+        r.bc_kind = prob.bc_kind
+        if prob.bc_state is not None:
+            for v in range(8):
+                r.bc_state8[v] = float(prob.bc_state[v])
+        r.final_T = prob.final_T if final_T is None else final_T
+        r.cfl = prob.cfl
+        r.use_oedg, r.use_ldf, r.ent_offset = int(use_oedg), int(use_ldf), int(ent_offset)
+        r.arrival = float(arrival)
+        r.u0 = u0.ctypes.data
+        avg = None
+        if want_avg:
+            avg = np.empty((8, nx + 2, ny + 2), order="F")
+            r.u_avg_out = avg.ctypes.data
+        self._keep.append((u0, avg))
+        _check("mhd_server_submit", self.lib.mhd_server_submit(self.h, C.byref(r)))
+        return avg
+
+    def run(self, max_seconds=0.0):
+        _check("mhd_server_run", self.lib.mhd_server_run(self.h, float(max_seconds)))
+
+    def results(self):
+        n = C.c_int()
+        self.lib.mhd_server_results(self.h, None, 0, C.byref(n))
+        arr = (capi.RequestResult * max(1, n.value))()
+        self.lib.mhd_server_results(self.h, arr, n.value, C.byref(n))
+        return [arr[i].as_dict() for i in range(n.value)]
+
+    def pending(self):
+        q, a, u = C.c_int(), C.c_int(), C.c_size_t()
+        self.lib.mhd_server_pending(self.h, C.byref(q), C.byref(a), C.byref(u))
+        return dict(queued=q.value, active=a.value, used_bytes=u.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -34,6 +34,28 @@ class Status(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
 
 
+class Request(C.Structure):
+    """mhd_request"""
+    _fields_ = [("id", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("p", C.c_int),
+                ("rknstg", C.c_int), ("left", C.c_double), ("right", C.c_double),
+                ("bottom", C.c_double), ("top", C.c_double), ("gamma", C.c_double),
+                ("bc_kind", C.c_int), ("pad_", C.c_int), ("bc_state8", C.c_double * 8),
+                ("final_T", C.c_double), ("cfl", C.c_double), ("use_oedg", C.c_int),
+                ("use_ldf", C.c_int), ("ent_offset", C.c_int), ("pad2_", C.c_int),
+                ("arrival", C.c_double), ("u0", C.c_void_p), ("u_avg_out", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    """mhd_request_result"""
+    _fields_ = [("id", C.c_longlong), ("arrival", C.c_double), ("admitted", C.c_double),
+                ("finished", C.c_double), ("t", C.c_double), ("steps", C.c_longlong),
+                ("retries", C.c_longlong), ("done", C.c_int), ("flags", C.c_int),
+                ("error", C.c_int), ("pad_", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _vp = C.c_void_p
@@ -64,6 +86,20 @@ SIGNATURES = {
     "mhd_gpu_advance": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(Status)]),
     "mhd_gpu_get_status": (C.c_int, [_vp, C.POINTER(Status)]),
     "mhd_gpu_state_device_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_dp)]),
+    "mhd_batch_create": (C.c_int, [C.POINTER(_vp)]),
+    "mhd_batch_destroy": (C.c_int, [_vp]),
+    "mhd_batch_add": (C.c_int, [_vp, _vp]),
+    "mhd_batch_remove": (C.c_int, [_vp, _vp]),
+    "mhd_batch_size": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "mhd_batch_advance": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
+    "mhd_batch_member_status": (C.c_int, [_vp, _vp, C.POINTER(Status)]),
+    "mhd_gpu_footprint": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+    "mhd_server_create": (C.c_int, [C.c_size_t, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "mhd_server_submit": (C.c_int, [_vp, C.POINTER(Request)]),
+    "mhd_server_run": (C.c_int, [_vp, C.c_double]),
+    "mhd_server_pending": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
+    "mhd_server_results": (C.c_int, [_vp, C.POINTER(RequestResult), C.c_int, C.POINTER(C.c_int)]),
+    "mhd_server_destroy": (C.c_int, [_vp]),
     "mhd_gpu_semidiscretize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                  C.c_double, _vp, _vp, _dp, _vp]),
 }

@@ -67,6 +67,37 @@ struct Geo {
   const double* ldfA;  // dense LDF nodal operator (2n^2 x 2n^2, column-major), device memory
 };
 
+// One solver instance as the batched kernels see it (a device-resident table entry).
+struct InstDesc {
+  Geo g;
+  double* u[6];   // slot 0 = u_con, s = uRK_con(:,s)
+  double* ut[6];  // 1..R
+  double* u_avg;
+  double* sig_x;
+  double* sig_y;
+  double* partial;
+  double* ent_partial;
+  double* cell_ent_DG;
+  double* cell_ent_FV;
+  unsigned char* cell_ent_nan;
+  Ctrl* ctrl;
+  int use_oedg, use_ldf, ent_offset, R;
+  int nblk_avg;    // pp_avg_ldf chunks of this instance (partial sums)
+  int nseg_limit;  // pp_limit segments of this instance (entropy partials)
+};
+
+// Batched kernels see a group's work of one kind as the concatenation of every member's items;
+// pref[m] is the first item of member m (pref[0] = 0, pref[n] = total).  Member of item w:
+__device__ __forceinline__ int batch_member(const int* __restrict__ pref, int n, int w) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(pref + mid) <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // ---- order-preserving encodings of doubles for atomicMax / atomicMin --------------------------
 __device__ __forceinline__ unsigned long long ord_enc(double x) {
   long long b = __double_as_longlong(x);

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <new>
 
@@ -98,7 +99,33 @@ int init_device_tables(int dev) {
   CK(cudaFuncSetAttribute(residual_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
   CK(cudaFuncSetAttribute(residual_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
   CK(cudaFuncSetAttribute(residual_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual_batched<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual_batched<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual_batched<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
   g_dev_init[dev] = true;
+  return MHD_OK;
+}
+
+// Instance buffers come from one memory pool per device that keeps freed memory reserved
+// (release threshold = all), so creating and destroying instances in a serving loop neither
+// pays cudaMalloc/cudaFree nor synchronises the device.
+cudaMemPool_t g_pool[kMaxDevices];
+bool g_pool_ready[kMaxDevices];
+
+int device_pool(int dev, cudaMemPool_t* pool) {
+  std::lock_guard<std::mutex> lk(g_init_mutex);
+  if (!g_pool_ready[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    CK(cudaMemPoolCreate(&g_pool[dev], &props));
+    unsigned long long thr = ~0ULL;
+    CK(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &thr));
+    g_pool_ready[dev] = true;
+  }
+  *pool = g_pool[dev];
   return MHD_OK;
 }
 
@@ -225,16 +252,20 @@ int build_step_graph(mhd_gpu* h) {
 void free_all(mhd_gpu* h) {
   if (!h) return;
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  cudaStream_t fs = h->own_stream;  // stream-ordered frees back into the device pool
   for (int s = 0; s < 6; ++s) {
-    if (h->u[s]) cudaFree(h->u[s]);
-    if (h->ut[s]) cudaFree(h->ut[s]);
+    if (h->u[s]) cudaFreeAsync(h->u[s], fs);
+    if (h->ut[s]) cudaFreeAsync(h->ut[s], fs);
   }
   void* ptrs[] = {h->u_avg, h->staging, h->ldfA, h->sig_x, h->sig_y, h->partial, h->ent_partial,
                   h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan, h->ctrl};
   for (void* p : ptrs)
-    if (p) cudaFree(p);
-  if (h->ctrl_host) cudaFreeHost(h->ctrl_host);
-  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (p) cudaFreeAsync(p, fs);
+  if (fs) {
+    cudaStreamSynchronize(fs);
+    cudaStreamDestroy(fs);
+  }
+  std::free(h->ctrl_host);
 }
 
 }  // namespace
@@ -302,15 +333,21 @@ int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, doub
   h->hx = (right - left) / nx;  // DG_solver.f90:93-94
   h->hy = (top - bottom) / ny;
   for (int v = 0; v < 8; ++v) h->bc_state[v] = bc_state8 ? bc_state8[v] : 0.0;
-#define ALLOC(ptr, bytes_)                                               \
-  do {                                                                   \
-    size_t b_ = (size_t)(bytes_);                                        \
-    if (cudaMalloc((void**)&(ptr), b_ ? b_ : 16) != cudaSuccess) {       \
-      free_all(h);                                                       \
-      delete h;                                                          \
-      return MHD_ERR_CUDA;                                               \
-    }                                                                    \
-    h->bytes += b_;                                                      \
+  cudaMemPool_t pool;
+  if (device_pool(h->device, &pool) || cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return MHD_ERR_CUDA;
+  }
+  h->stream = h->own_stream;
+#define ALLOC(ptr, bytes_)                                                                   \
+  do {                                                                                       \
+    size_t b_ = (size_t)(bytes_);                                                            \
+    if (cudaMallocFromPoolAsync((void**)&(ptr), b_ ? b_ : 16, pool, h->own_stream) != cudaSuccess) { \
+      free_all(h);                                                                           \
+      delete h;                                                                              \
+      return MHD_ERR_CUDA;                                                                   \
+    }                                                                                        \
+    h->bytes += b_;                                                                          \
   } while (0)
   const size_t sb = sizeof(double) * (size_t)n_state(h), tb = sizeof(double) * (size_t)n_ut(h);
   for (int s = 0; s <= rknstg; ++s) ALLOC(h->u[s], sb);
@@ -330,13 +367,12 @@ int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, doub
   ALLOC(h->cell_ent_nan, nelg);
   ALLOC(h->ctrl, sizeof(Ctrl));
 #undef ALLOC
-  if (cudaMallocHost((void**)&h->ctrl_host, sizeof(Ctrl)) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  h->ctrl_host = static_cast<Ctrl*>(std::calloc(1, sizeof(Ctrl)));
+  if (!h->ctrl_host) {
     free_all(h);
     delete h;
     return MHD_ERR_CUDA;
   }
-  h->stream = h->own_stream;
   // NaN-filled state, as the reference allocates with ieee_signaling_nan (DG_solver.f90:56,68-71)
   for (int s = 0; s <= rknstg; ++s) cudaMemsetAsync(h->u[s], 0xFF, sb, h->stream);
   for (int s = 1; s <= rknstg; ++s) cudaMemsetAsync(h->ut[s], 0xFF, tb, h->stream);
@@ -376,7 +412,10 @@ int mhd_gpu_set_stream(mhd_gpu_t* h, void* stream) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(h->stream));
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
-  h->solve_ready = 0;  // the step graph is recaptured on the new stream
+  if (h->step_exec) {  // recaptured on the new stream by the next advance
+    cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+  }
   return MHD_OK;
 }
 
@@ -554,8 +593,10 @@ int mhd_gpu_solve_begin(mhd_gpu_t* h, double final_T, double cfl, int use_oedg, 
   *h->ctrl_host = c;
   CK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  rc = build_step_graph(h);
-  if (rc) return rc;
+  if (h->step_exec) {  // the step graph is (re)captured lazily by the first advance
+    cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+  }
   h->solve_ready = 1;
   return MHD_OK;
 }
@@ -581,6 +622,10 @@ int mhd_gpu_advance(mhd_gpu_t* h, long long max_steps, int check_every, mhd_gpu_
   if (check_every <= 0) check_every = 16;
   rc = read_ctrl(h);
   if (rc) return rc;
+  if (!h->step_exec) {
+    rc = build_step_graph(h);
+    if (rc) return rc;
+  }
   const long long start = h->ctrl_host->steps;
   const long long target = (max_steps > 0) ? start + max_steps : 0x7fffffffffffffffLL;
   rc = set_step_limit(h, target);
@@ -695,3 +740,6 @@ extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, 
   }
   return MHD_OK;
 }
+
+#include "batch_impl.cuh"
+#include "server_impl.cuh"

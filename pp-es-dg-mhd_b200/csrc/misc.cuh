@@ -9,12 +9,10 @@ enum BcKind : int { BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_FIXED = 2, BC_XEXTRA
 
 // Ghost-ring fill (problems.f90:312-423,597-654).  One thread per ghost value; corners untouched.
 template <int P>
-__global__ void __launch_bounds__(256) bc_kernel(double* __restrict__ u, Geo g, const Ctrl* ctrl, int gate) {
+__device__ __forceinline__ void bc_value(double* __restrict__ u, const Geo& g, long long it) {
   constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
-  if (!gate_open(ctrl, gate)) return;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long nghost = 2LL * (nx + ny);
-  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (it >= nghost * EB) return;
   const int ge = (int)(it / EB), vi = (int)(it - (long long)ge * EB);
   const int v = vi / NN, q = vi - v * NN, k = q % N, l = q / N;
@@ -50,24 +48,40 @@ __global__ void __launch_bounds__(256) bc_kernel(double* __restrict__ u, Geo g, 
   u[dst] = u[((long long)sj * NXG + si) * EB + v * NN + sq];
 }
 
+template <int P>
+__global__ void __launch_bounds__(256) bc_kernel(double* __restrict__ u, Geo g, const Ctrl* ctrl, int gate) {
+  if (!gate_open(ctrl, gate)) return;
+  bc_value<P>(u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// many instances: items = every member's blocks of 256 ghost values
+template <int P>
+__global__ void __launch_bounds__(256) bc_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                                                  const int* __restrict__ nwork, const int* __restrict__ ninst,
+                                                  int slot, int gate) {
+  const int nw = *nwork, n = *ninst;
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate)) continue;
+    bc_value<P>(d.u[slot], d.g, (long long)chunk * 256 + threadIdx.x);
+  }
+}
+
 // SSP-RK stage update (drive.f90:130-275) on interior elements, rounded exactly as written
 // (explicit _rn intrinsics: no fused multiply-add contraction).
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 
 template <int EB>
-__global__ void __launch_bounds__(256)
-    combine_kernel(const double* __restrict__ u0, const double* __restrict__ r1, const double* __restrict__ r2,
-                   const double* __restrict__ r3, const double* __restrict__ r4,
-                   const double* __restrict__ k1, const double* __restrict__ k2, const double* __restrict__ k3,
-                   const double* __restrict__ k4, const double* __restrict__ k5, double* __restrict__ out,
-                   int nx, int ny, int R, int stage, const double* __restrict__ dt_ptr, double dt_arg,
-                   const Ctrl* ctrl, int gate) {
-  if (!gate_open(ctrl, gate)) return;
+__device__ __forceinline__ void combine_value(
+    const double* __restrict__ u0, const double* __restrict__ r1, const double* __restrict__ r2,
+    const double* __restrict__ r3, const double* __restrict__ r4, const double* __restrict__ k1,
+    const double* __restrict__ k2, const double* __restrict__ k3, const double* __restrict__ k4,
+    const double* __restrict__ k5, double* __restrict__ out, int nx, int ny, int R, int stage, double dt,
+    long long it) {
   const long long n = (long long)nx * ny * EB;
-  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (it >= n) return;
-  const double dt = dt_ptr ? *dt_ptr : dt_arg;
   const long long e = it / EB;
   const int c = (int)(it - e * EB);
   const int j = 1 + (int)(e / nx), i = 1 + (int)(e - (long long)(j - 1) * nx);
@@ -96,6 +110,35 @@ __global__ void __launch_bounds__(256)
     }
   }
   out[gi] = val;
+}
+
+template <int EB>
+__global__ void __launch_bounds__(256)
+    combine_kernel(const double* __restrict__ u0, const double* __restrict__ r1, const double* __restrict__ r2,
+                   const double* __restrict__ r3, const double* __restrict__ r4,
+                   const double* __restrict__ k1, const double* __restrict__ k2, const double* __restrict__ k3,
+                   const double* __restrict__ k4, const double* __restrict__ k5, double* __restrict__ out,
+                   int nx, int ny, int R, int stage, const double* __restrict__ dt_ptr, double dt_arg,
+                   const Ctrl* ctrl, int gate) {
+  if (!gate_open(ctrl, gate)) return;
+  const double dt = dt_ptr ? *dt_ptr : dt_arg;
+  combine_value<EB>(u0, r1, r2, r3, r4, k1, k2, k3, k4, k5, out, nx, ny, R, stage, dt,
+                    (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// many instances: items = every member's blocks of 256 values; dt from each member's control block
+template <int EB>
+__global__ void __launch_bounds__(256) combine_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                                                       const int* __restrict__ nwork, const int* __restrict__ ninst,
+                                                       int stage, int gate) {
+  const int nw = *nwork, n = *ninst;
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate)) continue;
+    combine_value<EB>(d.u[0], d.u[1], d.u[2], d.u[3], d.u[4], d.ut[1], d.ut[2], d.ut[3], d.ut[4], d.ut[5],
+                      d.u[stage], d.g.nx, d.g.ny, d.R, stage, d.ctrl->dt, (long long)chunk * 256 + threadIdx.x);
+  }
 }
 
 // Fortran layout (8, n, n, E) <-> element-blocked layout [E][8][n*n].  E = element count.
@@ -149,7 +192,7 @@ __device__ __forceinline__ double powi_d(double x, int n) {
 }
 
 // Start of one try of a time step (drive.f90:93-105).  Decodes the last residual's dt_lim.
-__global__ void ctl_step_begin(Ctrl* c) {
+__device__ __forceinline__ void ctl_step_begin_body(Ctrl* c) {
   if (c->pending_dtlim) {
     c->dt_lim = dec_dtlim(c->dt_lim_bits);
     c->pending_dtlim = 0;
@@ -175,7 +218,7 @@ __global__ void ctl_step_begin(Ctrl* c) {
 }
 
 // dt of this try (drive.f90:107-120)
-__global__ void ctl_dt(Ctrl* c) {
+__device__ __forceinline__ void ctl_dt_body(Ctrl* c) {
   if (c->pending_dtlim) {
     c->dt_lim = dec_dtlim(c->dt_lim_bits);
     c->pending_dtlim = 0;
@@ -197,7 +240,7 @@ __global__ void ctl_dt(Ctrl* c) {
 }
 
 // pseudo-time of stage s (drive.f90:142-267), computed before the stage's combine
-__global__ void ctl_stage_time(Ctrl* c, int R, int s) {
+__device__ __forceinline__ void ctl_stage_time_body(Ctrl* c, int R, int s) {
   if (c->state != ST_RUN) return;
   const double t = c->t, dt = c->dt;
   double* tr = c->t_rk;
@@ -234,7 +277,7 @@ __global__ void ctl_stage_time(Ctrl* c, int R, int s) {
 
 // after post_process of a stage (drive.f90:285-298): inadmissible average -> abandon the try;
 // otherwise account the limiter count and arm the dt_lim reduction of the coming residual.
-__global__ void ctl_stage_end(Ctrl* c) {
+__device__ __forceinline__ void ctl_stage_end_body(Ctrl* c) {
   if (c->state != ST_RUN) return;
   if (c->pp_relimit) {
     c->flags |= 2;  // MHD_FLAG_PP_RELIMIT (the reference stops the program)
@@ -253,7 +296,7 @@ __global__ void ctl_stage_end(Ctrl* c) {
 
 // end of a try: accept (drive.f90:304-312) or prepare the re-try.  dt_lim is the value of the
 // last residual that ran, as in the reference, where every DG_semidiscretize overwrites it.
-__global__ void ctl_step_end(Ctrl* c, int R) {
+__device__ __forceinline__ void ctl_step_end_body(Ctrl* c, int R) {
   if (c->pending_dtlim) {
     c->dt_lim = dec_dtlim(c->dt_lim_bits);
     c->pending_dtlim = 0;
@@ -268,6 +311,35 @@ __global__ void ctl_step_end(Ctrl* c, int R) {
   c->try_num = 0;
   if (c->last_step) c->done = 1;
   c->state = ST_IDLE;
+}
+
+__global__ void ctl_step_begin(Ctrl* c) { ctl_step_begin_body(c); }
+__global__ void ctl_dt(Ctrl* c) { ctl_dt_body(c); }
+__global__ void ctl_stage_time(Ctrl* c, int R, int s) { ctl_stage_time_body(c, R, s); }
+__global__ void ctl_stage_end(Ctrl* c) { ctl_stage_end_body(c); }
+__global__ void ctl_step_end(Ctrl* c, int R) { ctl_step_end_body(c, R); }
+
+// the same decisions for every instance of a batch, one thread each
+enum CtlOp : int { CTL_STEP_BEGIN = 0, CTL_DT = 1, CTL_STAGE_TIME = 2, CTL_STAGE_END = 3, CTL_STEP_END = 4 };
+__global__ void ctl_batched(const InstDesc* __restrict__ insts, const int* __restrict__ ninst, int op, int R, int s) {
+  const int n = *ninst;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Ctrl* c = insts[i].ctrl;
+    switch (op) {
+      case CTL_STEP_BEGIN: ctl_step_begin_body(c); break;
+      case CTL_DT: ctl_dt_body(c); break;
+      case CTL_STAGE_TIME: ctl_stage_time_body(c, R, s); break;
+      case CTL_STAGE_END: ctl_stage_end_body(c); break;
+      default: ctl_step_end_body(c, R); break;
+    }
+  }
+}
+
+// status of every instance of a batch into one contiguous array (one copy to the host)
+__global__ void ctl_gather_batched(const InstDesc* __restrict__ insts, const int* __restrict__ ninst,
+                                   Ctrl* __restrict__ out) {
+  const int n = *ninst;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = *insts[i].ctrl;
 }
 
 }  // namespace mhd

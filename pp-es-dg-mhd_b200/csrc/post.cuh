@@ -25,19 +25,164 @@ struct PPCfg {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Zhang-Shu positivity (DG_solver.f90:528-603), entropy-offset limiting (:606-633) and the cell
+// entropy (:635-649) of the elements a CTA holds in shared memory (s_u [e][var][node], s_avg
+// [e][8]).  Node-parallel: node pressures and entropies take one thread per node; the per-element
+// decisions take one lane per element; the rare re-limit loop stays serial per element.
+// mask (may be NULL = all) selects the elements to limit; cell-entropy arrays are indexed from
+// ebase; the CTA's entropy partial (elements in order) goes to *ent_out.
+// ---------------------------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ void limit_elements(double* s_u, const double* s_avg, const unsigned char* mask, int ne,
+                                               long long ebase, const Geo& g, Ctrl* ctrl, int ent_offset,
+                                               int comput_ent, const double* __restrict__ cell_ent_DG,
+                                               const double* __restrict__ cell_ent_FV,
+                                               const unsigned char* __restrict__ cell_ent_nan,
+                                               double* __restrict__ ent_out) {
+  using C = PPCfg<P>;
+  constexpr int N = C::N, NN = C::NN, EB = C::EB, TE = C::TE;
+  constexpr double BIG = 1.7976931348623157e308;
+  __shared__ double l_nd[TE * NN];
+  __shared__ double l_thd[TE], l_thp[TE];
+  __shared__ int l_cnt;
+  const int tid = threadIdx.x;
+  const double gamma = g.gamma;
+  const DegConst& dc = c_deg[P];
+  if (tid == 0) l_cnt = 0;
+  // density: theta from the minimum nodal density (DG_solver.f90:538-553)
+  if (tid < ne) {
+    double th = -1.0;
+    if (!mask || mask[tid]) {
+      const double* x = s_u + tid * EB;
+      double den_min = BIG;
+      for (int q = 0; q < NN; ++q) den_min = fmin(den_min, x[q]);
+      if (den_min < PP_EPS) {
+        const double da = s_avg[tid * 8];
+        th = fmax(fmin((da - PP_EPS) / (da - den_min), 1.0), 0.0);
+      }
+    }
+    l_thd[tid] = th;
+  }
+  __syncthreads();
+  for (int it = tid; it < ne * NN; it += PP_NT) {
+    const int e = it / NN, q = it - e * NN;
+    const double th = l_thd[e];
+    if (th >= 0.0) {
+      const double a0 = s_avg[e * 8];
+      double x = s_u[e * EB + q];
+      x = a0 + th * (x - a0);
+      s_u[e * EB + q] = fmax(x, PP_EPS);
+    }
+  }
+  __syncthreads();
+  // pressure: nodal pressures in parallel, theta from their minimum (DG_solver.f90:556-571)
+  for (int it = tid; it < ne * NN; it += PP_NT) {
+    const int e = it / NN, q = it - e * NN;
+    if (mask && !mask[e]) continue;
+    const double* x = s_u + e * EB + q;
+    l_nd[it] = prs_of(x[0], x[NN], x[2 * NN], x[3 * NN], x[4 * NN], x[5 * NN], x[6 * NN], x[7 * NN], gamma);
+  }
+  __syncthreads();
+  if (tid < ne) {
+    double th = -1.0;
+    if (!mask || mask[tid]) {
+      double pmin = BIG;
+      for (int q = 0; q < NN; ++q) pmin = fmin(pmin, l_nd[tid * NN + q]);
+      if (pmin < PP_EPS) {
+        const double* a = s_avg + tid * 8;
+        const double pa = prs_of(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], gamma);
+        th = fmax(fmin((pa - PP_EPS) / (pa - pmin), 1.0), 0.0);
+      }
+      if (l_thd[tid] >= 0.0 || th >= 0.0) atomicAdd(&l_cnt, 1);  // neg_node (DG_solver.f90:602)
+    }
+    l_thp[tid] = th;
+  }
+  __syncthreads();
+  for (int it = tid; it < ne * EB; it += PP_NT) {
+    const int e = it / EB;
+    const double th = l_thp[e];
+    if (th >= 0.0) {
+      const double a = s_avg[e * 8 + (it - e * EB) / NN];
+      s_u[it] = a + th * (s_u[it] - a);
+    }
+  }
+  __syncthreads();
+  if (tid < ne) {
+    double* x = s_u + tid * EB;
+    const double* a = s_avg + tid * 8;
+    double theta = l_thp[tid];
+    if (theta >= 0.0) {  // re-check after the FP-inexact theta (DG_solver.f90:573-599), rare
+      for (int it_count = 0;; ++it_count) {  // bounded: at most two extra shrinks
+        double prs_min = BIG;
+        for (int q = 0; q < NN; ++q)
+          prs_min = fmin(prs_min, prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma));
+        if (!(prs_min < 0.99 * PP_EPS)) break;
+        if (it_count > 1) {
+          atomicOr(&ctrl->pp_relimit, 1);
+          break;
+        }
+        theta = 0.6 * theta;
+        for (int v = 0; v < 8; ++v)
+          for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + theta * (x[v * NN + q] - a[v]);
+      }
+    }
+    const long long ce = ebase + tid;
+    if (ent_offset && (!mask || mask[tid]) && !cell_ent_nan[ce]) {  // DG_solver.f90:606-633
+      const double old = cell_ent_DG[ce], eavg = cell_ent_FV[ce];
+      double nw = 0.0;
+      for (int l = 0; l < N; ++l)
+        for (int k = 0; k < N; ++k) {
+          const int q = k + N * l;
+          const double pq = fmax(prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma), PP_EPS);
+          nw = nw + (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[q], pq, gamma);
+        }
+      if (nw > old) {
+        const double th = fmax(fmin((old - eavg) / (nw - eavg), 1.0), 0.0);
+        for (int v = 0; v < 8; ++v)
+          for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + th * (x[v * NN + q] - a[v]);
+      }
+    }
+  }
+  __syncthreads();
+  if (comput_ent) {  // DG_solver.f90:635-649
+    for (int it = tid; it < ne * NN; it += PP_NT) {
+      const int e = it / NN, q = it - e * NN;
+      if (mask && !mask[e]) continue;
+      const int k = q % N, l = q / N;
+      const double* x = s_u + e * EB + q;
+      const double pq = fmax(prs_of(x[0], x[NN], x[2 * NN], x[3 * NN], x[4 * NN], x[5 * NN], x[6 * NN], x[7 * NN], gamma), PP_EPS);
+      l_nd[it] = (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[0], pq, gamma);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double tot = 0.0;
+      for (int e = 0; e < ne; ++e) {
+        if (mask && !mask[e]) continue;
+        double ce = 0.0;
+        for (int q = 0; q < NN; ++q) ce = ce + l_nd[e * NN + q];
+        tot = tot + ce;
+      }
+      *ent_out = tot;
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && l_cnt) atomicAdd(&ctrl->num_negcell, l_cnt);
+}
+
+// ---------------------------------------------------------------------------------------------
 // loop 1: averages + admissibility + LDF.  A CTA owns TE consecutive element blocks of the
 // ghosted grid (one contiguous run of memory).
 // ---------------------------------------------------------------------------------------------
 template <int P>
-__global__ void __launch_bounds__(PP_NT)
-    pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
-                      int gate, int apply_ldf, int need_global, int ent_offset,
-                      double* __restrict__ partial_sum,     // [gridDim.x][8]
-                      double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
-                      unsigned char* __restrict__ cell_ent_nan) {
+__device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg,
+                                                 const Geo& g, Ctrl* ctrl, long long chunk, int apply_ldf,
+                                                 int need_global, int ent_offset,
+                                                 double* __restrict__ partial_out,  // 8 doubles
+                                                 double* __restrict__ cell_ent_DG,
+                                                 double* __restrict__ cell_ent_FV,
+                                                 unsigned char* __restrict__ cell_ent_nan) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, TE = C::TE;
-  if (!gate_open(ctrl, gate)) return;
   __shared__ __align__(16) double s_u[TE * EB];
   __shared__ double s_out[TE * N2];
   __shared__ double s_avg[TE * 8];
@@ -47,7 +192,7 @@ __global__ void __launch_bounds__(PP_NT)
   const int tid = threadIdx.x;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long total = (long long)NXG * (ny + 2);
-  const long long e0 = (long long)blockIdx.x * TE;
+  const long long e0 = chunk * TE;
   const int ne = (int)min((long long)TE, total - e0);
   const DegConst& dc = c_deg[P];
 
@@ -157,7 +302,7 @@ __global__ void __launch_bounds__(PP_NT)
       double sacc = 0.0;
       for (int e = 0; e < ne; ++e)
         if (s_inner[e]) sacc = sacc + (g.hx * g.hy) * s_avg[e * 8 + tid];
-      partial_sum[blockIdx.x * 8 + tid] = sacc;
+      partial_out[tid] = sacc;
     }
     // per-variable max and min of the post-LDF interior node values
     double vmax[8], vmin[8];
@@ -203,12 +348,40 @@ __global__ void __launch_bounds__(PP_NT)
   }
 }
 
+template <int P>
+__global__ void __launch_bounds__(PP_NT)
+    pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
+                      int gate, int apply_ldf, int need_global, int ent_offset,
+                      double* __restrict__ partial_sum,  // [gridDim.x][8]
+                      double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
+                      unsigned char* __restrict__ cell_ent_nan) {
+  if (!gate_open(ctrl, gate)) return;
+  pp_avg_ldf_chunk<P>(u, u_avg, g, ctrl, blockIdx.x, apply_ldf, need_global, ent_offset,
+                      partial_sum + (long long)blockIdx.x * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan);
+}
+
+// many instances: items = every member's chunks; slot = the stage state; `final` selects the
+// final-stage form (OEDG global reductions for instances that use OEDG)
+template <int P>
+__global__ void __launch_bounds__(PP_NT)
+    pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+  const int nw = *nwork, n = *ninst;
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate)) continue;
+    pp_avg_ldf_chunk<P>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, d.use_oedg && final,
+                        d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
+                        d.cell_ent_nan);
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // global average (fixed-order sum of block partials) and u_vari_global.  One CTA.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) pp_reduce_kernel(const double* __restrict__ partial, int nblk,
-                                                        Ctrl* ctrl, int gate) {
-  if (!gate_open(ctrl, gate)) return;
+__device__ __forceinline__ void pp_reduce_body(const double* __restrict__ partial, int nblk, Ctrl* ctrl) {
   __shared__ double s[8][256];
   const int tid = threadIdx.x;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -232,20 +405,35 @@ __global__ void __launch_bounds__(256) pp_reduce_kernel(const double* __restrict
   }
 }
 
+__global__ void __launch_bounds__(256) pp_reduce_kernel(const double* __restrict__ partial, int nblk,
+                                                        Ctrl* ctrl, int gate) {
+  if (!gate_open(ctrl, gate)) return;
+  pp_reduce_body(partial, nblk, ctrl);
+}
+
+// many instances: CTA per instance (persistent over the instance list)
+__global__ void __launch_bounds__(256) pp_reduce_batched(const InstDesc* __restrict__ insts,
+                                                         const int* __restrict__ ninst, int final, int gate) {
+  const int n = *ninst;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const InstDesc& d = insts[i];
+    if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
+    pp_reduce_body(d.partial, d.nblk_avg, d.ctrl);
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // OEDG face jump indicators.  One thread per (face, variable).  x faces first, then y faces.
 //   sigsum = sum_{kk,ll} (2m+1) h^m / (2 max(2p-1,1) kk! ll!) * <0.5 w, |d^kk_x d^ll_y jump|>
 // ---------------------------------------------------------------------------------------------
 template <int P>
-__global__ void __launch_bounds__(256)
-    pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
-                     double* __restrict__ sig_x, double* __restrict__ sig_y) {
+__device__ __forceinline__ void pp_sigsum_item(const double* __restrict__ u, const Geo& g, long long it,
+                                               double* __restrict__ sig_x, double* __restrict__ sig_y) {
   constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
-  if (!gate_open(ctrl, gate)) return;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long nfx = (long long)(nx + 1) * ny * 8;
   const long long nfy = (long long)nx * (ny + 1) * 8;
-  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (it >= nfx + nfy) return;
   const DegConst& dc = c_deg[P];
   const int denom_base = 2 * max(2 * P - 1, 1);
@@ -372,37 +560,53 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <int P>
+__global__ void __launch_bounds__(256)
+    pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
+                     double* __restrict__ sig_x, double* __restrict__ sig_y) {
+  if (!gate_open(ctrl, gate)) return;
+  pp_sigsum_item<P>(u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x, sig_x, sig_y);
+}
+
+// many instances: items = every member's blocks of 256 (face, variable) pairs
+template <int P>
+__global__ void __launch_bounds__(256)
+    pp_sigsum_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+  const int nw = *nwork, n = *ninst;
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
+    pp_sigsum_item<P>(d.u[slot], d.g, (long long)chunk * 256 + threadIdx.x, d.sig_x, d.sig_y);
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // loop 3: OEDG damping, positivity, entropy offset, entropy.  A CTA owns TE consecutive
 // interior elements of one row j (a contiguous run of memory).
 // ---------------------------------------------------------------------------------------------
 template <int P>
-__global__ void __launch_bounds__(PP_NT)
-    pp_limit_kernel(double* __restrict__ u, const double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
-                    int gate, int apply_oedg, const double* __restrict__ dt_ptr, double oedg_dt_arg,
-                    int ent_offset, int comput_ent, const double* __restrict__ sig_x,
-                    const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
-                    const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
-                    double* __restrict__ ent_partial, double* __restrict__ accept_dst) {
+__device__ __forceinline__ void pp_limit_segment(
+    double* __restrict__ u, const double* __restrict__ u_avg, const Geo& g, Ctrl* ctrl, int seg, int jrow,
+    int apply_oedg, double oedg_dt, int ent_offset, int comput_ent, const double* __restrict__ sig_x,
+    const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
+    const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
+    double* __restrict__ ent_out, double* __restrict__ accept_dst) {
   using C = PPCfg<P>;
-  constexpr int N = C::N, NN = C::NN, EB = C::EB, TE = C::TE;
-  if (!gate_open(ctrl, gate)) return;
+  constexpr int NN = C::NN, EB = C::EB, TE = C::TE;
   if (ctrl->neg_avg) return;  // the reference skips loop 3 once neg_avg is set (DG_solver.f90:431)
   __shared__ __align__(16) double s_u[TE * EB];
   __shared__ double s_avg[TE * 8];
   __shared__ double s_nd[TE * NN * 2];  // per-node scratch (wave speeds, pressures, entropies)
   __shared__ double s_theta[TE];
-  __shared__ int s_cnt;
   const int tid = threadIdx.x;
   const int nx = g.nx, NXG = nx + 2;
-  const int j = 1 + blockIdx.y;
-  const int i0 = 1 + blockIdx.x * TE;
+  const int j = 1 + jrow;
+  const int i0 = 1 + seg * TE;
   const int ne = min(TE, nx - i0 + 1);
   const long long ebase = (long long)j * NXG + i0;
-  const DegConst& dc = c_deg[P];
   const double gamma = g.gamma;
-  const double oedg_dt = dt_ptr ? *dt_ptr : oedg_dt_arg;
-  if (tid == 0) s_cnt = 0;
   for (int it = tid; it < ne * EB / 2; it += PP_NT)
     reinterpret_cast<double2*>(s_u)[it] = reinterpret_cast<const double2*>(u + ebase * EB)[it];
   for (int it = tid; it < ne * 8; it += PP_NT) s_avg[it] = u_avg[ebase * 8 + it];
@@ -454,101 +658,53 @@ __global__ void __launch_bounds__(PP_NT)
     __syncthreads();
   }
 
-  // Zhang-Shu positivity (DG_solver.f90:528-603); one thread per element, nodes in shared memory
-  if (tid < ne) {
-    const int e = tid;
-    double* x = s_u + e * EB;
-    const double* a = s_avg + e * 8;
-    bool neg_node = false;
-    double theta = 0.0;
-    const double den_avg = a[0];
-    const double prs_avg = prs_of(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], gamma);
-    double den_min = 1.7976931348623157e308;
-    for (int q = 0; q < NN; ++q) den_min = fmin(den_min, x[q]);
-    if (den_min < PP_EPS) {
-      neg_node = true;
-      theta = fmax(fmin((den_avg - PP_EPS) / (den_avg - den_min), 1.0), 0.0);
-      for (int q = 0; q < NN; ++q) x[q] = a[0] + theta * (x[q] - a[0]);
-      for (int q = 0; q < NN; ++q) x[q] = fmax(x[q], PP_EPS);
-    }
-    double prs_min = 1.7976931348623157e308;
-    for (int q = 0; q < NN; ++q)
-      prs_min = fmin(prs_min, prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma));
-    if (prs_min < PP_EPS) {
-      neg_node = true;
-      theta = fmax(fmin((prs_avg - PP_EPS) / (prs_avg - prs_min), 1.0), 0.0);
-      for (int v = 0; v < 8; ++v)
-        for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + theta * (x[v * NN + q] - a[v]);
-      for (int it_count = 0;; ++it_count) {  // bounded: at most two extra shrinks
-        prs_min = 1.7976931348623157e308;
-        for (int q = 0; q < NN; ++q)
-          prs_min = fmin(prs_min, prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma));
-        if (!(prs_min < 0.99 * PP_EPS)) break;
-        if (it_count > 1) {
-          atomicOr(&ctrl->pp_relimit, 1);
-          break;
-        }
-        theta = 0.6 * theta;
-        for (int v = 0; v < 8; ++v)
-          for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + theta * (x[v * NN + q] - a[v]);
-      }
-    }
-    if (neg_node) atomicAdd(&s_cnt, 1);
-    if (ent_offset) {  // DG_solver.f90:606-633
-      const long long ce = ebase + e;
-      if (!cell_ent_nan[ce]) {
-        const double old = cell_ent_DG[ce], eavg = cell_ent_FV[ce];
-        double nw = 0.0;
-        for (int l = 0; l < N; ++l)
-          for (int k = 0; k < N; ++k) {
-            const int q = k + N * l;
-            const double pq = fmax(prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma), PP_EPS);
-            nw = nw + (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[q], pq, gamma);
-          }
-        if (nw > old) {
-          const double th = fmax(fmin((old - eavg) / (nw - eavg), 1.0), 0.0);
-          for (int v = 0; v < 8; ++v)
-            for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + th * (x[v * NN + q] - a[v]);
-        }
-      }
-    }
-  }
-  __syncthreads();
-
-  if (comput_ent) {  // DG_solver.f90:635-649
-    for (int it = tid; it < ne * NN; it += PP_NT) {
-      const int e = it / NN, q = it - e * NN;
-      const int k = q % N, l = q / N;
-      const double* x = s_u + e * EB + q;
-      const double pq = fmax(prs_of(x[0], x[NN], x[2 * NN], x[3 * NN], x[4 * NN], x[5 * NN], x[6 * NN], x[7 * NN], gamma), PP_EPS);
-      s_nd[it] = (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[0], pq, gamma);
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double tot = 0.0;
-      for (int e = 0; e < ne; ++e) {
-        double ce = 0.0;
-        for (int q = 0; q < NN; ++q) ce = ce + s_nd[e * NN + q];
-        tot = tot + ce;
-      }
-      ent_partial[blockIdx.y * gridDim.x + blockIdx.x] = tot;
-    }
-  }
+  limit_elements<P>(s_u, s_avg, nullptr, ne, ebase, g, ctrl, ent_offset, comput_ent, cell_ent_DG, cell_ent_FV,
+                    cell_ent_nan, ent_out);
 
   for (int it = tid; it < ne * EB / 2; it += PP_NT) {
     const double2 val = reinterpret_cast<const double2*>(s_u)[it];
     reinterpret_cast<double2*>(u + ebase * EB)[it] = val;
     if (accept_dst) reinterpret_cast<double2*>(accept_dst + ebase * EB)[it] = val;
   }
-  __syncthreads();
-  if (tid == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
+}
+
+template <int P>
+__global__ void __launch_bounds__(PP_NT)
+    pp_limit_kernel(double* __restrict__ u, const double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
+                    int gate, int apply_oedg, const double* __restrict__ dt_ptr, double oedg_dt_arg,
+                    int ent_offset, int comput_ent, const double* __restrict__ sig_x,
+                    const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
+                    const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
+                    double* __restrict__ ent_partial, double* __restrict__ accept_dst) {
+  if (!gate_open(ctrl, gate)) return;
+  const double oedg_dt = dt_ptr ? *dt_ptr : oedg_dt_arg;
+  pp_limit_segment<P>(u, u_avg, g, ctrl, blockIdx.x, blockIdx.y, apply_oedg, oedg_dt, ent_offset, comput_ent,
+                      sig_x, sig_y, cell_ent_DG, cell_ent_FV, cell_ent_nan,
+                      ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst);
+}
+
+// many instances: items = every member's row segments (row-major); the final stage applies OEDG
+// (if the instance uses it), computes the entropy and writes the accepted interior into slot 0
+template <int P>
+__global__ void __launch_bounds__(PP_NT)
+    pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                     const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+  const int nw = *nwork, n = *ninst;
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate)) continue;
+    const int nseg = (d.g.nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE;
+    const int seg = local % nseg, row = local / nseg;
+    pp_limit_segment<P>(d.u[slot], d.u_avg, d.g, d.ctrl, seg, row, d.use_oedg && final, d.ctrl->dt,
+                        d.ent_offset, final, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
+                        d.ent_partial + local, final ? d.u[0] : nullptr);
+    __syncthreads();
+  }
 }
 
 // total entropy = fixed-order sum of the per-CTA partials.  One CTA.
-__global__ void __launch_bounds__(256) pp_entsum_kernel(const double* __restrict__ partial, int nblk,
-                                                        Ctrl* ctrl, int gate) {
-  if (!gate_open(ctrl, gate)) return;
-  if (ctrl->neg_avg) return;
+__device__ __forceinline__ void pp_entsum_body(const double* __restrict__ partial, int nblk, Ctrl* ctrl) {
   __shared__ double s[256];
   const int tid = threadIdx.x;
   double acc = 0.0;
@@ -560,6 +716,24 @@ __global__ void __launch_bounds__(256) pp_entsum_kernel(const double* __restrict
     __syncthreads();
   }
   if (tid == 0) ctrl->tot_ent = s[0];
+}
+
+__global__ void __launch_bounds__(256) pp_entsum_kernel(const double* __restrict__ partial, int nblk,
+                                                        Ctrl* ctrl, int gate) {
+  if (!gate_open(ctrl, gate)) return;
+  if (ctrl->neg_avg) return;
+  pp_entsum_body(partial, nblk, ctrl);
+}
+
+__global__ void __launch_bounds__(256) pp_entsum_batched(const InstDesc* __restrict__ insts,
+                                                         const int* __restrict__ ninst, int gate) {
+  const int n = *ninst;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const InstDesc& d = insts[i];
+    if (!gate_open(d.ctrl, gate) || d.ctrl->neg_avg) continue;
+    pp_entsum_body(d.ent_partial, d.nseg_limit, d.ctrl);
+    __syncthreads();
+  }
 }
 
 }  // namespace mhd

@@ -70,15 +70,15 @@ __device__ __forceinline__ void pair_ab(int idx, int& a, int& b) {
 }
 __device__ __forceinline__ int pair_index(int a, int b) { return a * (a - 1) / 2 + b; }
 
+// One tile of the residual: elements (tile_x*TX + 1 .. , tile_y*TY + 1 .. ) of the instance
+// described by (u, ut, g, ctrl).  All threads of the CTA call it with the same arguments.
 template <int P>
-__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
-    residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl,
-                    int gate) {
+__device__ __forceinline__ void residual_tile(const double* __restrict__ u, double* __restrict__ ut,
+                                              const Geo& g, Ctrl* ctrl, int tile_x, int tile_y,
+                                              double* sm) {
   using L = ResLayout<P>;
   constexpr int N = L::N, NN = L::NN, EB = L::EB, TX = L::TX, TY = L::TY, TE = L::TE;
   constexpr int NT = ResCfg<P>::NT;
-  if (!gate_open(ctrl, gate)) return;
-  extern __shared__ __align__(16) double sm[];
   double* s_cons = sm + L::O_CONS;
   double* s_prim = sm + L::O_PRIM;
   double* s_hxl = sm + L::O_HXL;
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
 
   const int tid = threadIdx.x;
   const int nx = g.nx, ny = g.ny;
-  const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;  // first interior element
+  const int i0 = 1 + tile_x * TX, j0 = 1 + tile_y * TY;  // first interior element
   const int W = min(TX, nx - i0 + 1), H = min(TY, ny - j0 + 1);
   const long long rowstride = (long long)(nx + 2) * EB;
   const double gamma = g.gamma;
@@ -394,6 +394,33 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
         dst[c] = reinterpret_cast<const double2*>(s_cons + r * TX * EB)[c];
       }
     }
+  }
+}
+
+// single instance: one CTA per tile
+template <int P>
+__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
+    residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate) {
+  if (!gate_open(ctrl, gate)) return;
+  extern __shared__ __align__(16) double sm[];
+  residual_tile<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm);
+}
+
+// many instances of degree P: a persistent grid walks every member's tiles (row-major per member);
+// the state is slot `src`, the result goes to ut[dst]
+template <int P>
+__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
+    residual_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                     const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate) {
+  extern __shared__ __align__(16) double sm[];
+  const int nw = *nwork, n = *ninst;
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate)) continue;
+    const int ntx = (d.g.nx + ResCfg<P>::TX - 1) / ResCfg<P>::TX;
+    residual_tile<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm);
+    __syncthreads();  // the next tile reuses shared memory
   }
 }
 

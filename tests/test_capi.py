@@ -11,7 +11,7 @@ from conftest import ROOT
 def declared_functions():
     src = open(os.path.join(ROOT, "include", "mhd_gpu.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(mhd_gpu_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(mhd_(?:gpu|batch|server)_\w+)\s*\(", src)))
 
 
 def test_every_declared_symbol_is_exported(pkg):

@@ -67,7 +67,7 @@ def test_gpu_matches_fixture(pkg, path):
     with pkg.DGSolver.for_problem(prob, nx, ny, p) as g:
         g.upload_state(0, d["u_bc"])
         dl = g.semidiscretize(1, 0)
-        assert rel_l1(g.download_ut(1), d["ut"]).max() <= 1e-12
+        assert rel_l1(g.download_ut(1), d["ut"], floor_frac=1e-2).max() <= 1e-12
         assert abs(dl - float(d["dt_lim"])) <= 1e-13 * float(d["dt_lim"])
         g.upload_state(1, d["u1_in"])
         pp = g.post_process(1, 1, 1, float(d["pp_dt"]), 0, 1)

@@ -1,0 +1,95 @@
+"""Batched instances (GPU): every member of a batch computes exactly what it computes alone.
+
+The batch runs the same kernel bodies over a flattened work list of all members' tiles, so the
+identity is bitwise: a member advanced K tries inside a mixed batch (different degrees, problems,
+gammas, mesh sizes) has the same state, time and entropy as the same instance advanced K steps on
+its own.  Members can join and leave between advances.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIX = [("ot2pi", 20, 2, 1.0, None), ("rotor", 17, 1, 1.3, None), ("ot2pi", 12, 3, 0.7, 1.4),
+       ("rotor", 24, 3, 0.6, 5.0 / 3.0), ("blast", 16, 2, 1.0, None), ("vortex", 10, 1, 1.0, None)]
+
+
+def _make(pkg, name, n, p, amp, gamma):
+    prob = pkg.problems.make(name, gamma=gamma, amp=amp) if name != "vortex" else pkg.problems.make(name)
+    u0 = prob.initial_state(n, n, p)
+    s = pkg.DGSolver.for_problem(prob, n, n, p)
+    s.upload_state(0, u0)
+    s.solve_begin(prob.final_T, prob.cfl)
+    return s
+
+
+def test_batch_members_identical_to_solo_runs(pkg):
+    K = 6
+    solo = []
+    for spec in MIX:
+        s = _make(pkg, *spec)
+        st = s.advance(K)
+        solo.append((s.download_state(0), st))
+        s.close()
+    with pkg.Batch() as b:
+        members = [_make(pkg, *spec) for spec in MIX]
+        for m in members:
+            b.add(m)
+        assert len(b) == len(MIX)
+        b.advance(K)
+        for m, (u_ref, st_ref) in zip(members, solo):
+            st = b.status(m)
+            assert st["retries"] == 0 and st_ref["retries"] == 0
+            assert st["steps"] == st_ref["steps"] == K
+            assert st["t"] == st_ref["t"] and st["dt_lim"] == st_ref["dt_lim"]
+            assert st["tot_ent"] == st_ref["tot_ent"]
+            assert st["num_negcell_total"] == st_ref["num_negcell_total"]
+        for m in list(members):
+            b.remove(m)
+        for m, (u_ref, _) in zip(members, solo):
+            np.testing.assert_array_equal(m.download_state(0), u_ref)
+            m.close()
+
+
+def test_members_join_and_leave(pkg):
+    with pkg.Batch() as b:
+        a = _make(pkg, "ot2pi", 16, 2, 1.0, None)
+        c = _make(pkg, "rotor", 12, 1, 1.0, None)
+        b.add(a)
+        b.add(c)
+        b.advance(3)
+        b.remove(c)
+        d = _make(pkg, "ot2pi", 14, 3, 0.8, None)  # a new degree group joins
+        b.add(d)
+        b.advance(2)
+        assert b.status(a)["steps"] == 5 and b.status(d)["steps"] == 2
+        assert c.status()["steps"] == 3  # the removed member kept its state
+        c.advance(2)  # and runs on its own again
+        assert c.status()["steps"] == 5
+        ref = _make(pkg, "rotor", 12, 1, 1.0, None)
+        ref.advance(5)
+        np.testing.assert_array_equal(c.download_state(0), ref.download_state(0))
+        for s in (a, d):
+            b.remove(s)
+            s.close()
+        c.close()
+        ref.close()
+
+
+def test_finished_members_idle(pkg):
+    with pkg.Batch() as b:
+        prob = pkg.problems.make("ot2pi")
+        s = pkg.DGSolver.for_problem(prob, 8, 8, 1)
+        s.upload_state(0, prob.initial_state(8, 8, 1))
+        s.solve_begin(0.02, prob.cfl)  # a few steps to the end time
+        b.add(s)
+        for _ in range(50):
+            if b.advance(4) == 0:
+                break
+        st = b.status(s)
+        assert st["done"] == 1 and abs(st["t"] - 0.02) < 1e-15
+        steps = st["steps"]
+        b.advance(3)
+        assert b.status(s)["steps"] == steps
+        b.remove(s)
+        s.close()
