@@ -254,13 +254,16 @@ def serve(pkg, reqs, batched, budget, tries_per_round=2):
     srv.run()
     wall = time.perf_counter() - t0
     res = srv.results()
+    stats = srv.stats()
     srv.close()
     tts = np.array([x["finished"] - x["arrival"] for x in res])
     makespan = max(x["finished"] for x in res) - min(x["arrival"] for x in res)
     ok = sum(1 for x in res if x["done"] == 1 and x["flags"] == 0 and x["error"] == 0)
     return {"solves_per_s": len(res) / makespan, "p50_tts_s": float(np.percentile(tts, 50)),
             "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok, "requests": len(reqs),
-            "wall_s": wall, "steps": int(sum(x["steps"] for x in res))}
+            "wall_s": wall, "steps": int(sum(x["steps"] for x in res)),
+            "host_s": {k: round(stats[k], 4) for k in ("admit_s", "launch_s", "wait_s", "retire_s", "idle_s")},
+            "rounds": stats["rounds"], "graph_captures": stats["graph_captures"]}
 
 
 def serve_leg(pkg, n_req=48, rate=400.0, seed=7, n_lo=32, n_hi=192, t_scale=0.2, budget=64 << 30):

@@ -181,7 +181,12 @@ int mhd_batch_size(const mhd_batch_t *b, int *n);
  * a re-try, or nothing once done), then a refresh of every member's status; *n_active (may be
  * NULL) = members neither done nor failed. */
 int mhd_batch_advance(mhd_batch_t *b, int tries, int *n_active);
-/* a member's status as of the last mhd_batch_advance */
+/* mhd_batch_advance in two halves, so that the host can work while a round runs: _launch queues
+ * the round and returns; _wait blocks until it has finished and refreshes the statuses.  Between
+ * the two, members can be neither added nor removed (MHD_ERR_STATE). */
+int mhd_batch_launch(mhd_batch_t *b, int tries);
+int mhd_batch_wait(mhd_batch_t *b, int *n_active);
+/* a member's status as of the last completed round */
 int mhd_batch_member_status(mhd_batch_t *b, mhd_gpu_t *h, mhd_gpu_status *st);
 
 /* ---- serving ------------------------------------------------------------------------------ */
@@ -218,7 +223,10 @@ typedef struct mhd_request_result {
 /* A request loop with continuous batching: runs are admitted when they have arrived and their
  * footprint fits the HBM budget (at most max_active at once), all active runs advance together in
  * one batch (tries_per_round batched tries between polls), finished runs retire and free their
- * memory.  batched = 0 serves the same queue one plain run at a time (the comparison point). */
+ * memory.  batched = 0 serves the same queue one plain run at a time (the comparison point).
+ * The budget is reserved on the device when the server is created (one allocation; a budget the
+ * device cannot hold returns MHD_ERR_UNSUPPORTED) and every run's buffers are carved from it, so
+ * the loop itself makes no device allocation call.  Admissions overlap the round in flight. */
 typedef struct mhd_server mhd_server_t;
 int mhd_server_create(size_t hbm_budget_bytes, int max_active, int tries_per_round, int batched,
                       mhd_server_t **out);
@@ -227,6 +235,18 @@ int mhd_server_submit(mhd_server_t *s, const mhd_request *r);
 int mhd_server_run(mhd_server_t *s, double max_seconds);
 int mhd_server_pending(const mhd_server_t *s, int *queued, int *active, size_t *used_bytes);
 int mhd_server_results(const mhd_server_t *s, mhd_request_result *out, int cap, int *n);
+/* where the loop's host time went (wall seconds, summed over every mhd_server_run) */
+typedef struct mhd_server_stats {
+  long long rounds;          /* batched rounds launched (plain mode: runs executed) */
+  long long admitted, retired;
+  long long graph_captures;  /* batch graph (re)captures */
+  double admit_s;            /* creating instances, uploading, solve_begin */
+  double launch_s;           /* queueing rounds */
+  double wait_s;             /* blocked on the device */
+  double retire_s;           /* downloading results, freeing instances, batch membership */
+  double idle_s;             /* nothing active and nothing arrived */
+} mhd_server_stats;
+int mhd_server_get_stats(const mhd_server_t *s, mhd_server_stats *out);
 int mhd_server_destroy(mhd_server_t *s);
 
 /* ---- allocation-free residual ------------------------------------------------------------ */

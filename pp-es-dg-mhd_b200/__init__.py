@@ -247,6 +247,16 @@ class Batch:
         _check("mhd_batch_advance", self.lib.mhd_batch_advance(self.h, int(tries), C.byref(n)))
         return n.value
 
+    def launch(self, tries=1):
+        """queue `tries` batched tries and return at once (membership is frozen until wait)"""
+        _check("mhd_batch_launch", self.lib.mhd_batch_launch(self.h, int(tries)))
+
+    def wait(self):
+        """finish the launched round; returns the number of members neither done nor failed"""
+        n = C.c_int()
+        _check("mhd_batch_wait", self.lib.mhd_batch_wait(self.h, C.byref(n)))
+        return n.value
+
     def status(self, solver):
         st = Status()
         rc = self.lib.mhd_batch_member_status(self.h, solver.h, C.byref(st))
@@ -325,6 +335,11 @@ class Server:
         arr = (capi.RequestResult * max(1, n.value))()
         self.lib.mhd_server_results(self.h, arr, n.value, C.byref(n))
         return [arr[i].as_dict() for i in range(n.value)]
+
+    def stats(self):
+        st = capi.ServerStats()
+        _check("mhd_server_get_stats", self.lib.mhd_server_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
 
     def pending(self):
         q, a, u = C.c_int(), C.c_int(), C.c_size_t()

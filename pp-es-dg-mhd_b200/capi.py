@@ -56,6 +56,16 @@ class RequestResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
 
 
+class ServerStats(C.Structure):
+    """mhd_server_stats"""
+    _fields_ = [("rounds", C.c_longlong), ("admitted", C.c_longlong), ("retired", C.c_longlong),
+                ("graph_captures", C.c_longlong), ("admit_s", C.c_double), ("launch_s", C.c_double),
+                ("wait_s", C.c_double), ("retire_s", C.c_double), ("idle_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _vp = C.c_void_p
@@ -92,6 +102,8 @@ SIGNATURES = {
     "mhd_batch_remove": (C.c_int, [_vp, _vp]),
     "mhd_batch_size": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "mhd_batch_advance": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
+    "mhd_batch_launch": (C.c_int, [_vp, C.c_int]),
+    "mhd_batch_wait": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "mhd_batch_member_status": (C.c_int, [_vp, _vp, C.POINTER(Status)]),
     "mhd_gpu_footprint": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
     "mhd_server_create": (C.c_int, [C.c_size_t, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
@@ -99,6 +111,7 @@ SIGNATURES = {
     "mhd_server_run": (C.c_int, [_vp, C.c_double]),
     "mhd_server_pending": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
     "mhd_server_results": (C.c_int, [_vp, C.POINTER(RequestResult), C.c_int, C.POINTER(C.c_int)]),
+    "mhd_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
     "mhd_server_destroy": (C.c_int, [_vp]),
     "mhd_gpu_semidiscretize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                  C.c_double, _vp, _vp, _dp, _vp]),

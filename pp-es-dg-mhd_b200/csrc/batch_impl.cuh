@@ -19,8 +19,12 @@ enum WorkKind { WK_RES = 0, WK_AVG, WK_SIG, WK_LIM, WK_CMB, WK_BC, WK_COUNT };
 
 // One group's device table, one allocation, uploaded with one copy:
 //   InstDesc insts[cap] | int total[WK_COUNT] | int ninst | int pref[WK_COUNT][cap + 1]
+constexpr int kIdleRounds = 64;  // rounds an empty group is kept in the graph
+constexpr int kMinCap = 16;      // members a group's table holds before it first grows
+
 struct BatchGroup {
   int p = 0, R = 0;
+  int idle_rounds = 0;  // rounds launched since the group last had a member
   std::vector<mhd_gpu*> members;
   char* d_table = nullptr;
   int cap = 0;
@@ -40,9 +44,9 @@ int sm_count(int dev) {
 }  // namespace
 
 struct mhd_batch {
-  int device;
-  int nsm;
-  cudaStream_t stream;
+  int device = 0;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
   std::vector<BatchGroup> groups;
   std::vector<mhd_gpu*> members;  // in insertion order
   cudaGraphExec_t exec = nullptr;
@@ -55,6 +59,9 @@ struct mhd_batch {
   size_t cap_stage = 0;
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> ev;
+  cudaEvent_t join_ev = nullptr;  // orders a joining member's queued work before the next round
+  bool in_flight = false;         // a round was launched and not yet waited for
+  long long captures = 0;         // graph (re)captures so far
 };
 
 namespace {
@@ -102,21 +109,24 @@ void member_work(const mhd_gpu* h, long long* cnt, InstDesc& d) {
 
 // upload every group's table (one copy per group from pinned staging); grows buffers as needed
 int refresh_batch(mhd_batch* b) {
+  // an empty group stays in the graph (its launches find no work) until it has idled kIdleRounds
+  // rounds, so that runs of one degree coming and going do not re-capture the graph each time
   for (auto& g : b->groups)
-    if (g.members.empty()) {
+    if (g.members.empty() && g.idle_rounds > kIdleRounds) {
       if (g.d_table) cudaFree(g.d_table);
       g.d_table = nullptr;
       b->graph_stale = true;
     }
   b->groups.erase(std::remove_if(b->groups.begin(), b->groups.end(),
-                                 [](const BatchGroup& g) { return g.members.empty(); }),
+                                 [](const BatchGroup& g) { return !g.d_table && g.members.empty() && g.idle_rounds > kIdleRounds; }),
                   b->groups.end());
   size_t stage_need = 0;
   for (auto& g : b->groups) {
     const int n = (int)g.members.size();
+    if (n) g.idle_rounds = 0;
     if (n > g.cap || !g.d_table) {
       if (g.d_table) cudaFree(g.d_table);
-      g.cap = std::max(n, 2 * g.cap);
+      g.cap = std::max(std::max(n, kMinCap), 2 * g.cap);
       CK(cudaMalloc((void**)&g.d_table, g.table_bytes(g.cap)));
       b->graph_stale = true;
     }
@@ -168,43 +178,66 @@ int refresh_batch(mhd_batch* b) {
   return MHD_OK;
 }
 
+// persistent grid: every CTA the SMs can hold at once for this kernel
+template <class K>
+int full_grid(K kernel, int threads, size_t smem, int nsm) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * nsm;
+}
+
+struct BatchGrids {
+  int res, cmb, bc, avg, sig, lim;
+};
+
+// queried before a capture begins (the occupancy calculator is host-only work)
 template <int P>
-void enqueue_group_try(mhd_batch* b, BatchGroup& g, cudaStream_t st) {
+BatchGrids batch_grids(int nsm) {
+  constexpr int EB = 8 * (P + 1) * (P + 1);
+  BatchGrids gr;
+  gr.res = full_grid(residual_batched<P>, ResCfg<P>::NT, ResLayout<P>::BYTES, nsm);
+  gr.cmb = full_grid(combine_batched<EB>, 256, 0, nsm);
+  gr.bc = full_grid(bc_batched<P>, 256, 0, nsm);
+  gr.avg = full_grid(pp_avg_ldf_batched<P>, PP_NT, 0, nsm);
+  gr.sig = full_grid(pp_sigsum_batched<P>, 256, 0, nsm);
+  gr.lim = full_grid(pp_limit_batched<P>, PP_NT, 0, nsm);
+  return gr;
+}
+
+template <int P>
+void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaStream_t st) {
   constexpr int EB = 8 * (P + 1) * (P + 1);
   const int R = g.R;
   const int* tot = g.total();
   const int* ninst = g.ninst();
   InstDesc* in = g.insts();
-  const int grid_res = b->nsm * ResCfg<P>::MINB;
-  const int grid_pp = b->nsm * 4;
   const size_t smem = ResLayout<P>::BYTES;
+  const int grid_res = gr.res, grid_cmb = gr.cmb, grid_bc = gr.bc, grid_avg = gr.avg, grid_sig = gr.sig,
+            grid_lim = gr.lim;
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_BEGIN, R, 0);
   residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE);
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_DT, R, 0);
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_TIME, R, s);
-    combine_batched<EB><<<grid_pp, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
-    bc_batched<P><<<grid_pp, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
-    pp_avg_ldf_batched<P><<<grid_pp, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, fin, ST_RUN);
+    combine_batched<EB><<<grid_cmb, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
+    bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
+    pp_avg_ldf_batched<P><<<grid_avg, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, fin, ST_RUN);
     if (fin) {
       pp_reduce_batched<<<b->nsm, 256, 0, st>>>(in, ninst, fin, ST_RUN);
-      pp_sigsum_batched<P><<<grid_pp, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);
+      pp_sigsum_batched<P><<<grid_sig, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);
     }
-    pp_limit_batched<P><<<grid_pp, PP_NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
+    pp_limit_batched<P><<<grid_lim, PP_NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
     if (fin) pp_entsum_batched<<<b->nsm, 256, 0, st>>>(in, ninst, ST_RUN);
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_END, R, s);
-    bc_batched<P><<<grid_pp, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
+    bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
     residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, s, (s % R) + 1, ST_RUN);
   }
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_END, R, 0);
 }
 
 int capture_batch_graph(mhd_batch* b) {
-  if (b->exec) {
-    cudaGraphExecDestroy(b->exec);
-    b->exec = nullptr;
-  }
   while (b->branch.size() < b->groups.size()) {
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -215,32 +248,46 @@ int capture_batch_graph(mhd_batch* b) {
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     b->ev.push_back(e);
   }
-  cudaGraph_t graph;
+  const BatchGrids grids[3] = {batch_grids<1>(b->nsm), batch_grids<2>(b->nsm), batch_grids<3>(b->nsm)};
+  cudaGraph_t graph = nullptr;
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  CK(cudaEventRecord(b->ev[0], b->stream));
+  // every call below is recorded, not run; an error invalidates the capture, which still ends
+  cudaEventRecord(b->ev[0], b->stream);
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     cudaStream_t st = b->branch[gi];
-    CK(cudaStreamWaitEvent(st, b->ev[0], 0));
+    cudaStreamWaitEvent(st, b->ev[0], 0);
     BatchGroup& g = b->groups[gi];
     switch (g.p) {
-      case 1: enqueue_group_try<1>(b, g, st); break;
-      case 2: enqueue_group_try<2>(b, g, st); break;
-      default: enqueue_group_try<3>(b, g, st); break;
+      case 1: enqueue_group_try<1>(b, g, grids[0], st); break;
+      case 2: enqueue_group_try<2>(b, g, grids[1], st); break;
+      default: enqueue_group_try<3>(b, g, grids[2], st); break;
     }
-    CK(cudaEventRecord(b->ev[gi + 1], st));
-    CK(cudaStreamWaitEvent(b->stream, b->ev[gi + 1], 0));
+    cudaEventRecord(b->ev[gi + 1], st);
+    cudaStreamWaitEvent(b->stream, b->ev[gi + 1], 0);
   }
   cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
-  if (e != cudaSuccess) return MHD_ERR_CUDA;
-  e = cudaGraphInstantiate(&b->exec, graph, 0);
+  if (e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return MHD_ERR_CUDA;
+  }
+  if (b->exec) {  // same groups, new tables: update the executable graph in place
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(b->exec, graph, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+  }
+  e = b->exec ? cudaSuccess : cudaGraphInstantiate(&b->exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return MHD_ERR_CUDA;
   b->graph_stale = false;
   return MHD_OK;
 }
 
-// copy every member's control block into the members' host mirrors
-int gather_status(mhd_batch* b) {
+// copy every member's control block to the pinned host mirror (asynchronous)
+int enqueue_gather(mhd_batch* b) {
   int off = 0;
   for (auto& g : b->groups) {
     const int n = (int)g.members.size();
@@ -250,10 +297,51 @@ int gather_status(mhd_batch* b) {
   }
   CK(cudaGetLastError());
   if (off) CK(cudaMemcpyAsync(b->h_status, b->d_status, sizeof(Ctrl) * off, cudaMemcpyDeviceToHost, b->stream));
-  CK(cudaStreamSynchronize(b->stream));
-  off = 0;
+  return MHD_OK;
+}
+
+// after the stream is idle: hand each member its control block
+void unpack_gather(mhd_batch* b) {
+  int off = 0;
   for (auto& g : b->groups)
     for (mhd_gpu* h : g.members) *h->ctrl_host = b->h_status[off++];
+}
+
+int batch_launch(mhd_batch* b, int tries) {
+  if (b->in_flight) return MHD_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  if (b->dirty) {
+    int rc = refresh_batch(b);
+    if (rc) return rc;
+  }
+  if (!b->members.empty()) {
+    if (b->graph_stale) {
+      int rc = capture_batch_graph(b);
+      if (rc) return rc;
+      ++b->captures;
+    }
+    for (int t = 0; t < tries; ++t) CK(cudaGraphLaunch(b->exec, b->stream));
+    for (auto& g : b->groups)
+      if (g.members.empty() && ++g.idle_rounds > kIdleRounds) b->dirty = true;  // dropped at the next refresh
+  }
+  int rc = enqueue_gather(b);
+  if (rc) return rc;
+  b->in_flight = true;
+  return MHD_OK;
+}
+
+int batch_wait(mhd_batch* b, int* n_active) {
+  if (!b->in_flight) return MHD_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  b->in_flight = false;
+  CK(cudaStreamSynchronize(b->stream));
+  unpack_gather(b);
+  if (n_active) {
+    int a = 0;
+    for (mhd_gpu* h : b->members)
+      if (!h->ctrl_host->done && !(h->ctrl_host->flags & 0xE)) ++a;
+    *n_active = a;
+  }
   return MHD_OK;
 }
 
@@ -269,7 +357,9 @@ int mhd_batch_create(mhd_batch_t** out) {
   mhd_batch* b = new (std::nothrow) mhd_batch;
   if (!b) return MHD_ERR_INVALID;
   if (cudaGetDevice(&b->device) != cudaSuccess || init_device_tables(b->device) ||
-      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return MHD_ERR_CUDA;
   }
@@ -282,6 +372,7 @@ int mhd_batch_destroy(mhd_batch_t* b) {
   if (!b) return MHD_ERR_INVALID;
   cudaSetDevice(b->device);
   cudaStreamSynchronize(b->stream);
+  b->in_flight = false;
   for (mhd_gpu* h : b->members) h->stream = h->own_stream;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   for (auto& g : b->groups)
@@ -291,6 +382,7 @@ int mhd_batch_destroy(mhd_batch_t* b) {
   if (b->h_status) cudaFreeHost(b->h_status);
   for (auto s : b->branch) cudaStreamDestroy(s);
   for (auto e : b->ev) cudaEventDestroy(e);
+  if (b->join_ev) cudaEventDestroy(b->join_ev);
   cudaStreamDestroy(b->stream);
   delete b;
   return MHD_OK;
@@ -299,10 +391,12 @@ int mhd_batch_destroy(mhd_batch_t* b) {
 int mhd_batch_add(mhd_batch_t* b, mhd_gpu_t* h) {
   if (!b || !h) return MHD_ERR_INVALID;
   if (h->device != b->device) return MHD_ERR_INVALID;
-  if (!h->solve_ready) return MHD_ERR_STATE;
+  if (!h->solve_ready || b->in_flight) return MHD_ERR_STATE;
   if (std::find(b->members.begin(), b->members.end(), h) != b->members.end()) return MHD_ERR_STATE;
   CK(cudaSetDevice(b->device));
-  CK(cudaStreamSynchronize(h->stream));
+  // the batch stream waits (on the device) for the member's queued work
+  CK(cudaEventRecord(b->join_ev, h->stream));
+  CK(cudaStreamWaitEvent(b->stream, b->join_ev, 0));
   h->stream = b->stream;  // the batch drives the member from now on
   b->members.push_back(h);
   BatchGroup* grp = nullptr;
@@ -322,6 +416,7 @@ int mhd_batch_add(mhd_batch_t* b, mhd_gpu_t* h) {
 
 int mhd_batch_remove(mhd_batch_t* b, mhd_gpu_t* h) {
   if (!b || !h) return MHD_ERR_INVALID;
+  if (b->in_flight) return MHD_ERR_STATE;
   auto it = std::find(b->members.begin(), b->members.end(), h);
   if (it == b->members.end()) return MHD_ERR_STATE;
   CK(cudaSetDevice(b->device));
@@ -341,33 +436,25 @@ int mhd_batch_size(const mhd_batch_t* b, int* n) {
 
 int mhd_batch_advance(mhd_batch_t* b, int tries, int* n_active) {
   if (!b || tries < 0) return MHD_ERR_INVALID;
-  CK(cudaSetDevice(b->device));
-  if (b->dirty) {
-    int rc = refresh_batch(b);
-    if (rc) return rc;
-  }
-  if (!b->members.empty()) {
-    if (b->graph_stale) {
-      int rc = capture_batch_graph(b);
-      if (rc) return rc;
-    }
-    for (int t = 0; t < tries; ++t) CK(cudaGraphLaunch(b->exec, b->stream));
-  }
-  int rc = gather_status(b);
+  int rc = batch_launch(b, tries);
   if (rc) return rc;
-  if (n_active) {
-    int a = 0;
-    for (mhd_gpu* h : b->members)
-      if (!h->ctrl_host->done && !(h->ctrl_host->flags & 0x6)) ++a;
-    *n_active = a;
-  }
-  return MHD_OK;
+  return batch_wait(b, n_active);
+}
+
+int mhd_batch_launch(mhd_batch_t* b, int tries) {
+  if (!b || tries < 0) return MHD_ERR_INVALID;
+  return batch_launch(b, tries);
+}
+
+int mhd_batch_wait(mhd_batch_t* b, int* n_active) {
+  if (!b) return MHD_ERR_INVALID;
+  return batch_wait(b, n_active);
 }
 
 int mhd_batch_member_status(mhd_batch_t* b, mhd_gpu_t* h, mhd_gpu_status* st) {
   if (!b || !h || !st) return MHD_ERR_INVALID;
   if (std::find(b->members.begin(), b->members.end(), h) == b->members.end()) return MHD_ERR_STATE;
-  fill_status(h, st);  // as of the last mhd_batch_advance
+  fill_status(h, st);  // as of the last completed round
   return h->ctrl_host->flags;
 }
 

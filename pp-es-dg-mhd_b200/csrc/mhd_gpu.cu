@@ -44,6 +44,8 @@ struct mhd_gpu {
   Ctrl* ctrl;
   Ctrl* ctrl_host;  // pinned mirror
   size_t bytes;
+  void* block;      // the one device allocation every buffer above is carved from
+  bool owns_block;  // false: the block was lent by a server and goes back to it
   Geo geo;
   // device-resident driver
   int solve_ready;
@@ -63,6 +65,43 @@ bool g_dev_init[kMaxDevices];
     cudaError_t e_ = (call);                      \
     if (e_ != cudaSuccess) return MHD_ERR_CUDA;   \
   } while (0)
+
+// Where each buffer of an instance sits in its one device block (256-byte aligned pieces).
+struct InstLayout {
+  size_t u[6], ut[6], u_avg, staging, ldfA, sig_x, sig_y, partial, ent_partial, cell_ent_DG, cell_ent_FV,
+      cell_ent_nan, ctrl, total;
+};
+
+InstLayout inst_layout(int nx, int ny, int p, int R) {
+  InstLayout L;
+  std::memset(&L, 0, sizeof(L));
+  size_t off = 0;
+  auto take = [&off](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  const size_t eb = 8 * (size_t)(p + 1) * (p + 1);
+  const size_t nelg = (size_t)(nx + 2) * (ny + 2);
+  const size_t sb = sizeof(double) * nelg * eb, tb = sizeof(double) * (size_t)nx * ny * eb;
+  for (int s = 0; s <= R; ++s) L.u[s] = take(sb);
+  for (int s = 1; s <= R; ++s) L.ut[s] = take(tb);
+  L.u_avg = take(sizeof(double) * 8 * nelg);
+  L.staging = take(sb);
+  const size_t n2 = 2 * (size_t)(p + 1) * (p + 1);
+  L.ldfA = take(sizeof(double) * n2 * n2);
+  L.sig_x = take(sizeof(double) * 8 * (size_t)(nx + 1) * ny);
+  L.sig_y = take(sizeof(double) * 8 * (size_t)nx * (ny + 1));
+  const size_t te_min = 16;  // the smallest elements-per-CTA of the post-process kernels
+  L.partial = take(sizeof(double) * 8 * ((nelg + te_min - 1) / te_min + 1));
+  L.ent_partial = take(sizeof(double) * (((size_t)nx + te_min - 1) / te_min + 1) * ny);
+  L.cell_ent_DG = take(sizeof(double) * nelg);
+  L.cell_ent_FV = take(sizeof(double) * nelg);
+  L.cell_ent_nan = take(nelg);
+  L.ctrl = take(sizeof(Ctrl));
+  L.total = off;
+  return L;
+}
 
 long long n_state(const mhd_gpu* h) { return (long long)(h->nx + 2) * (h->ny + 2) * h->eb; }
 long long n_ut(const mhd_gpu* h) { return (long long)h->nx * h->ny * h->eb; }
@@ -252,15 +291,8 @@ int build_step_graph(mhd_gpu* h) {
 void free_all(mhd_gpu* h) {
   if (!h) return;
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
-  cudaStream_t fs = h->own_stream;  // stream-ordered frees back into the device pool
-  for (int s = 0; s < 6; ++s) {
-    if (h->u[s]) cudaFreeAsync(h->u[s], fs);
-    if (h->ut[s]) cudaFreeAsync(h->ut[s], fs);
-  }
-  void* ptrs[] = {h->u_avg, h->staging, h->ldfA, h->sig_x, h->sig_y, h->partial, h->ent_partial,
-                  h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan, h->ctrl};
-  for (void* p : ptrs)
-    if (p) cudaFreeAsync(p, fs);
+  cudaStream_t fs = h->own_stream;  // a stream-ordered free back into the device pool
+  if (h->block && h->owns_block) cudaFreeAsync(h->block, fs);
   if (fs) {
     cudaStreamSynchronize(fs);
     cudaStreamDestroy(fs);
@@ -294,8 +326,19 @@ int mhd_gpu_gll_tables(int p, double* x, double* w, double* M, double* Minv, dou
   return tables::gll(p, x, w, M, Minv, D, Pmn, Pnm) ? MHD_ERR_INVALID : MHD_OK;
 }
 
-int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, double right, double bottom,
-                   double top, double gamma, int bc_kind, const double* bc_state8, mhd_gpu_t** out) {
+}  // extern "C"
+
+namespace {
+
+// mhd_gpu_create.  With sync = false the set-up work stays queued on the instance's own stream.
+// u0 (may be NULL): an initial state in the Fortran layout, uploaded into slot 0.  Its host-to-device
+// copy and the LDF table's are queued before any kernel, so that (from pageable memory, where the
+// copy first waits for the stream's earlier work) the host never waits for the device.
+// block (may be NULL): device memory of at least inst_layout(...).total bytes lent by the caller,
+// which takes it back after mhd_gpu_destroy; NULL: one allocation from the device pool.
+int create_instance(int nx, int ny, int px, int py, int rknstg, double left, double right, double bottom,
+                    double top, double gamma, int bc_kind, const double* bc_state8, const double* u0, bool sync,
+                    void* block, mhd_gpu_t** out) {
   if (!out) return MHD_ERR_INVALID;
   *out = nullptr;
   if (nx < 2 || ny < 2 || !(right > left) || !(top > bottom) || !(gamma > 1.0)) return MHD_ERR_INVALID;
@@ -339,48 +382,53 @@ int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, doub
     return MHD_ERR_CUDA;
   }
   h->stream = h->own_stream;
-#define ALLOC(ptr, bytes_)                                                                   \
-  do {                                                                                       \
-    size_t b_ = (size_t)(bytes_);                                                            \
-    if (cudaMallocFromPoolAsync((void**)&(ptr), b_ ? b_ : 16, pool, h->own_stream) != cudaSuccess) { \
-      free_all(h);                                                                           \
-      delete h;                                                                              \
-      return MHD_ERR_CUDA;                                                                   \
-    }                                                                                        \
-    h->bytes += b_;                                                                          \
-  } while (0)
+  const InstLayout L = inst_layout(nx, ny, px, rknstg);
+  if (block) {
+    h->block = block;
+    h->owns_block = false;
+  } else {
+    if (cudaMallocFromPoolAsync(&h->block, L.total, pool, h->own_stream) != cudaSuccess) {
+      h->block = nullptr;
+      free_all(h);
+      delete h;
+      return MHD_ERR_CUDA;
+    }
+    h->owns_block = true;
+  }
+  h->bytes = L.total;
+  char* base = static_cast<char*>(h->block);
+  for (int s = 0; s <= rknstg; ++s) h->u[s] = reinterpret_cast<double*>(base + L.u[s]);
+  for (int s = 1; s <= rknstg; ++s) h->ut[s] = reinterpret_cast<double*>(base + L.ut[s]);
+  h->u_avg = reinterpret_cast<double*>(base + L.u_avg);
+  h->staging = reinterpret_cast<double*>(base + L.staging);
+  h->ldfA = reinterpret_cast<double*>(base + L.ldfA);
+  h->sig_x = reinterpret_cast<double*>(base + L.sig_x);
+  h->sig_y = reinterpret_cast<double*>(base + L.sig_y);
+  h->partial = reinterpret_cast<double*>(base + L.partial);
+  h->ent_partial = reinterpret_cast<double*>(base + L.ent_partial);
+  h->cell_ent_DG = reinterpret_cast<double*>(base + L.cell_ent_DG);
+  h->cell_ent_FV = reinterpret_cast<double*>(base + L.cell_ent_FV);
+  h->cell_ent_nan = reinterpret_cast<unsigned char*>(base + L.cell_ent_nan);
+  h->ctrl = reinterpret_cast<Ctrl*>(base + L.ctrl);
   const size_t sb = sizeof(double) * (size_t)n_state(h), tb = sizeof(double) * (size_t)n_ut(h);
-  for (int s = 0; s <= rknstg; ++s) ALLOC(h->u[s], sb);
-  for (int s = 1; s <= rknstg; ++s) ALLOC(h->ut[s], tb);
   const long long nelg = (long long)(nx + 2) * (ny + 2);
-  ALLOC(h->u_avg, sizeof(double) * 8 * nelg);
-  ALLOC(h->staging, sb);
   const int n2 = 2 * h->nn;
-  ALLOC(h->ldfA, sizeof(double) * n2 * n2);
-  ALLOC(h->sig_x, sizeof(double) * 8 * (size_t)(nx + 1) * ny);
-  ALLOC(h->sig_y, sizeof(double) * 8 * (size_t)nx * (ny + 1));
-  const int te_min = 16;
-  ALLOC(h->partial, sizeof(double) * 8 * (size_t)((nelg + te_min - 1) / te_min + 1));
-  ALLOC(h->ent_partial, sizeof(double) * (size_t)((nx + te_min - 1) / te_min + 1) * ny);
-  ALLOC(h->cell_ent_DG, sizeof(double) * nelg);
-  ALLOC(h->cell_ent_FV, sizeof(double) * nelg);
-  ALLOC(h->cell_ent_nan, nelg);
-  ALLOC(h->ctrl, sizeof(Ctrl));
-#undef ALLOC
   h->ctrl_host = static_cast<Ctrl*>(std::calloc(1, sizeof(Ctrl)));
   if (!h->ctrl_host) {
     free_all(h);
     delete h;
     return MHD_ERR_CUDA;
   }
+  if (u0) cudaMemcpyAsync(h->staging, u0, sb, cudaMemcpyHostToDevice, h->stream);
+  double A[32 * 32];
+  tables::ldf_nodal_operator(px, h->hx, h->hy, A);
+  cudaMemcpyAsync(h->ldfA, A, sizeof(double) * n2 * n2, cudaMemcpyHostToDevice, h->stream);
   // NaN-filled state, as the reference allocates with ieee_signaling_nan (DG_solver.f90:56,68-71)
   for (int s = 0; s <= rknstg; ++s) cudaMemsetAsync(h->u[s], 0xFF, sb, h->stream);
   for (int s = 1; s <= rknstg; ++s) cudaMemsetAsync(h->ut[s], 0xFF, tb, h->stream);
   cudaMemsetAsync(h->u_avg, 0xFF, sizeof(double) * 8 * nelg, h->stream);
   cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), h->stream);
-  double A[32 * 32];
-  tables::ldf_nodal_operator(px, h->hx, h->hy, A);
-  cudaMemcpyAsync(h->ldfA, A, sizeof(double) * n2 * n2, cudaMemcpyHostToDevice, h->stream);
+  if (u0) to_blocked_kernel<<<grid1d(nelg * h->eb, 256), 256, 0, h->stream>>>(h->staging, h->u[0], nelg, h->nn);
   h->geo.nx = nx;
   h->geo.ny = ny;
   h->geo.hx = h->hx;
@@ -389,13 +437,23 @@ int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, doub
   h->geo.bc_kind = bc_kind;
   for (int v = 0; v < 8; ++v) h->geo.bc_state[v] = h->bc_state[v];
   h->geo.ldfA = h->ldfA;
-  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+  if ((sync ? cudaStreamSynchronize(h->stream) : cudaGetLastError()) != cudaSuccess) {
     free_all(h);
     delete h;
     return MHD_ERR_CUDA;
   }
   *out = h;
   return MHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, double right, double bottom,
+                   double top, double gamma, int bc_kind, const double* bc_state8, mhd_gpu_t** out) {
+  return create_instance(nx, ny, px, py, rknstg, left, right, bottom, top, gamma, bc_kind, bc_state8, nullptr, true,
+                         nullptr, out);
 }
 
 int mhd_gpu_destroy(mhd_gpu_t* h) {
@@ -451,12 +509,12 @@ int mhd_gpu_ldf_operator(int p, double hx, double hy, double* A) {
   return tables::ldf_nodal_operator(p, hx, hy, A) ? MHD_ERR_INVALID : MHD_OK;
 }
 
-static int transfer_in(mhd_gpu* h, const double* src, double* dst, long long nelem) {
+static int transfer_in(mhd_gpu* h, const double* src, double* dst, long long nelem, bool sync = true) {
   const long long n = nelem * h->eb;
   CK(cudaMemcpyAsync(h->staging, src, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
   to_blocked_kernel<<<grid1d(n, 256), 256, 0, h->stream>>>(h->staging, dst, nelem, h->nn);
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(h->stream));
+  if (sync) CK(cudaStreamSynchronize(h->stream));
   return MHD_OK;
 }
 static int transfer_out(mhd_gpu* h, const double* src, double* dst, long long nelem) {

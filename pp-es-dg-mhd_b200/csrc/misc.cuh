@@ -197,7 +197,7 @@ __device__ __forceinline__ void ctl_step_begin_body(Ctrl* c) {
     c->dt_lim = dec_dtlim(c->dt_lim_bits);
     c->pending_dtlim = 0;
   }
-  if (c->done || (c->flags & 0x6) || c->steps >= c->step_limit) {  // finished, error, or step budget used
+  if (c->done || (c->flags & 0xE) || c->steps >= c->step_limit) {  // finished, error, or step budget used
     c->state = ST_IDLE;
     return;
   }
@@ -318,6 +318,29 @@ __global__ void ctl_dt(Ctrl* c) { ctl_dt_body(c); }
 __global__ void ctl_stage_time(Ctrl* c, int R, int s) { ctl_stage_time_body(c, R, s); }
 __global__ void ctl_stage_end(Ctrl* c) { ctl_stage_end_body(c); }
 __global__ void ctl_step_end(Ctrl* c, int R) { ctl_step_end_body(c, R); }
+
+// The starting control block of solve_execute (drive.f90:67-73) without a host round trip: the
+// initial post_process and residual ran just before on this stream, and their outputs (neg_avg,
+// tot_ent, the dt_lim reduction cell) become the first step's inputs.  An inadmissible initial
+// value sets MHD_FLAG_INIT_NEG_AVG, which every later try treats as a failed run.
+__global__ void ctl_solve_begin(Ctrl* c, double final_T, double cfl_total) {
+  const int neg = c->neg_avg;
+  const double te = c->tot_ent;
+  const unsigned long long bits = c->dt_lim_bits;
+  Ctrl z;
+  memset(&z, 0, sizeof(z));
+  z.final_T = final_T;
+  z.cfl_total = cfl_total;
+  z.state = ST_IDLE;
+  z.step_limit = 0x7fffffffffffffffLL;
+  if (neg) {
+    z.flags = 8;  // MHD_FLAG_INIT_NEG_AVG
+  } else {
+    z.dt_lim = dec_dtlim(bits);
+    z.tot_ent = te;
+  }
+  *c = z;
+}
 
 // the same decisions for every instance of a batch, one thread each
 enum CtlOp : int { CTL_STEP_BEGIN = 0, CTL_DT = 1, CTL_STAGE_TIME = 2, CTL_STAGE_END = 3, CTL_STEP_END = 4 };

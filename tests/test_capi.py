@@ -52,3 +52,27 @@ def test_create_rejects_bad_arguments_before_touching_a_device(pkg):
     assert lib.mhd_gpu_create(8, 8, 2, 2, 3, 1.0, 0.0, 0.0, 1.0, 1.4, 0, None, C.byref(h)) == pkg.capi.MHD_ERR_INVALID
     assert lib.mhd_gpu_create(8, 8, 2, 2, 3, 0.0, 1.0, 0.0, 1.0, 1.4, 2, None, C.byref(h)) == pkg.capi.MHD_ERR_INVALID
     assert not h.value
+
+
+def test_struct_layouts_match_the_header(pkg, tmp_path):
+    """the ctypes mirrors of the header's structs have the C sizes and field offsets (gcc-compiled probe)"""
+    import subprocess
+    cap = pkg.capi
+    structs = {"mhd_gpu_status": cap.Status, "mhd_request": cap.Request,
+               "mhd_request_result": cap.RequestResult, "mhd_server_stats": cap.ServerStats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "mhd_gpu.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)

@@ -93,3 +93,25 @@ def test_finished_members_idle(pkg):
         assert b.status(s)["steps"] == steps
         b.remove(s)
         s.close()
+
+
+def test_launch_then_wait_equals_advance(pkg):
+    a1, a2 = _make(pkg, "ot2pi", 16, 2, 1.0, None), _make(pkg, "rotor", 12, 3, 1.0, None)
+    r1, r2 = _make(pkg, "ot2pi", 16, 2, 1.0, None), _make(pkg, "rotor", 12, 3, 1.0, None)
+    with pkg.Batch() as b, pkg.Batch() as ref:
+        b.add(a1), b.add(a2), ref.add(r1), ref.add(r2)
+        b.launch(3)
+        with pytest.raises(pkg.MHDError):  # membership is frozen while a round is in flight
+            b.remove(a1)
+        assert b.wait() == 2
+        ref.advance(3)
+        for m, r in ((a1, r1), (a2, r2)):
+            assert b.status(m) == ref.status(r)
+        for s in (a1, a2):
+            b.remove(s)
+        for s in (r1, r2):
+            ref.remove(s)
+        np.testing.assert_array_equal(a1.download_state(0), r1.download_state(0))
+        np.testing.assert_array_equal(a2.download_state(0), r2.download_state(0))
+    for s in (a1, a2, r1, r2):
+        s.close()

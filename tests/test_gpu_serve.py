@@ -35,6 +35,9 @@ def test_served_results_identical_to_plain_runs(pkg, batched):
             assert r["steps"] == st["steps"] and r["t"] == st["t"]
             m = np.isfinite(ref_avg)
             np.testing.assert_array_equal(avgs[i][m], ref_avg[m])
+        st = srv.stats()
+        assert st["admitted"] == st["retired"] == len(REQS) and st["rounds"] >= 1
+        assert min(st[k] for k in ("admit_s", "launch_s", "wait_s", "retire_s", "idle_s")) >= 0.0
 
 
 def test_admission_respects_budget(pkg):
@@ -53,3 +56,20 @@ def test_admission_respects_budget(pkg):
         res = srv.results()
         assert len(res) == 5 and all(r["done"] == 1 for r in res)
         assert srv.pending()["used_bytes"] == 0
+
+
+@pytest.mark.parametrize("batched", [True, False])
+def test_inadmissible_initial_value_is_reported(pkg, batched):
+    """a run whose initial state has a negative cell-average density ends with
+    MHD_FLAG_INIT_NEG_AVG and no steps (drive.f90:70), next to a healthy run that completes"""
+    prob = pkg.problems.make("ot2pi")
+    good = prob.initial_state(10, 10, 2)
+    bad = good.copy(order="F")
+    bad[0, :, :, 4, 5] = -1.0
+    with pkg.Server(hbm_budget_bytes=8 << 30, tries_per_round=2, batched=batched) as srv:
+        srv.submit(0, prob, 10, 10, 2, bad, 0.0, final_T=0.01)
+        srv.submit(1, prob, 10, 10, 2, good, 0.0, final_T=0.01)
+        srv.run(max_seconds=120)
+        res = {r["id"]: r for r in srv.results()}
+    assert res[0]["flags"] & pkg.capi.MHD_FLAG_INIT_NEG_AVG and res[0]["steps"] == 0 and res[0]["done"] == 0
+    assert res[1]["done"] == 1 and res[1]["flags"] == 0
