@@ -124,36 +124,49 @@ __device__ __forceinline__ double ent_of(double rho, double prs, double gamma) {
   return -(rho * (log(prs) - gamma * log(rho)) / (gamma - 1.0));
 }
 
-// log_avg_divisor (DG_solver.f90:1652-1681): 0.5*(a+b)/ff is the logarithmic mean of a and b.
-__device__ __forceinline__ double log_avg_divisor(double LL, double RR) {
-  const double zeta = LL / RR;
-  const double f = (zeta - 1.0) / (zeta + 1.0);
-  const double u = f * f;
-  if (u < 1.4e-4) return 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0)));
-  return 0.5 * log(zeta) / f;
-}
-
 // Entropy-conservative two-point flux, x (DIR=0, DG_solver.f90:1570-1609) or y (DIR=1,
 // DG_solver.f90:1611-1650).  a, b = (rho, vx, vy, vz, bx, by, bz, beta).
+//
+// The reference forms rho_hat = rho_bar / ff(rho) and beta_hat = beta_bar / ff(beta) with
+// ff = log_avg_divisor (zeta = a/b, f = (zeta-1)/(zeta+1), the series when f^2 < 1.4e-4, else
+// 0.5 log(zeta)/f), then divides by beta_bar three times and by beta_hat once.  The same values
+// with fewer FP64 divisions, by algebra only:
+//   f = (a-b)/(a+b)                                  (= (zeta-1)/(zeta+1))
+//   series:  rho_hat = rho_bar / (1 + u/3 + u^2/5 + u^3/7),  u = f^2
+//   log:     rho_hat = rho_bar / (0.5 log(zeta)/f) = (a-b) / log(a/b)
+//   1/beta_hat = ff(beta) / beta_bar = ff(beta) * inv_bb,  inv_bb = 1/beta_bar
+// and every "/ beta_bar" becomes "* inv_bb".  Results agree with the reference's expression order
+// to a few ulp; the series/log branch is decided on the same u.
+__device__ __forceinline__ double series_divisor(double u) {
+  return 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0)));
+}
+
 template <int DIR>
 __device__ __forceinline__ void ec_flux(const double* a, const double* b, double gamma, double* f) {
-  const double rho_bar = 0.5 * (a[0] + b[0]);
+  const double rho_s = a[0] + b[0], beta_s = a[7] + b[7];
+  const double rho_bar = 0.5 * rho_s;
   const double vx_bar = 0.5 * (a[1] + b[1]);
   const double vy_bar = 0.5 * (a[2] + b[2]);
   const double vz_bar = 0.5 * (a[3] + b[3]);
   const double bx_bar = 0.5 * (a[4] + b[4]);
   const double by_bar = 0.5 * (a[5] + b[5]);
   const double bz_bar = 0.5 * (a[6] + b[6]);
-  const double beta_bar = 0.5 * (a[7] + b[7]);
+  const double inv_bb = 2.0 / beta_s;  // 1 / beta_bar
   const double v_sq_bar = 0.5 * ((a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) + (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]));
   const double b_sq_bar = 0.5 * ((a[4] * a[4] + a[5] * a[5] + a[6] * a[6]) + (b[4] * b[4] + b[5] * b[5] + b[6] * b[6]));
   const double bvx = 0.5 * (a[7] * a[1] + b[7] * b[1]);
   const double bvy = 0.5 * (a[7] * a[2] + b[7] * b[2]);
   const double bvz = 0.5 * (a[7] * a[3] + b[7] * b[3]);
-  const double rho_hat = rho_bar / log_avg_divisor(a[0], b[0]);
-  const double beta_hat = beta_bar / log_avg_divisor(a[7], b[7]);
-  const double ptot = 0.5 * (b_sq_bar + rho_bar / beta_bar);
-  const double ecoef = 0.5 * (1.0 / ((gamma - 1.0) * beta_hat) - v_sq_bar);
+  // logarithmic mean of rho
+  const double rho_d = a[0] - b[0];
+  const double fr = rho_d / rho_s, ur = fr * fr;
+  const double rho_hat = (ur < 1.4e-4) ? rho_bar / series_divisor(ur) : rho_d / log(a[0] / b[0]);
+  // divisor of the logarithmic mean of beta
+  const double beta_d = a[7] - b[7];
+  const double fb = beta_d * (0.5 * inv_bb), ub = fb * fb;
+  const double ffb = (ub < 1.4e-4) ? series_divisor(ub) : 0.5 * log(a[7] / b[7]) / fb;
+  const double ptot = 0.5 * (b_sq_bar + rho_bar * inv_bb);
+  const double ecoef = 0.5 * (ffb * inv_bb / (gamma - 1.0) - v_sq_bar);
   const double vb = vx_bar * bx_bar + vy_bar * by_bar + vz_bar * bz_bar;
   if (DIR == 0) {
     f[0] = rho_hat * vx_bar;
@@ -161,8 +174,8 @@ __device__ __forceinline__ void ec_flux(const double* a, const double* b, double
     f[2] = vy_bar * f[0] - bx_bar * by_bar;
     f[3] = vz_bar * f[0] - bx_bar * bz_bar;
     f[4] = 0.0;
-    f[5] = (bvx * by_bar - bvy * bx_bar) / beta_bar;
-    f[6] = (bvx * bz_bar - bvz * bx_bar) / beta_bar;
+    f[5] = (bvx * by_bar - bvy * bx_bar) * inv_bb;
+    f[6] = (bvx * bz_bar - bvz * bx_bar) * inv_bb;
     f[7] = ecoef * f[0] + (vx_bar * f[1] + vy_bar * f[2] + vz_bar * f[3]) +
            (bx_bar * f[4] + by_bar * f[5] + bz_bar * f[6]) - 0.5 * vx_bar * b_sq_bar + vb * bx_bar;
   } else {
@@ -170,9 +183,9 @@ __device__ __forceinline__ void ec_flux(const double* a, const double* b, double
     f[1] = vx_bar * f[0] - by_bar * bx_bar;
     f[2] = vy_bar * f[0] - by_bar * by_bar + ptot;
     f[3] = vz_bar * f[0] - by_bar * bz_bar;
-    f[4] = (bvy * bx_bar - bvx * by_bar) / beta_bar;
+    f[4] = (bvy * bx_bar - bvx * by_bar) * inv_bb;
     f[5] = 0.0;
-    f[6] = (bvy * bz_bar - bvz * by_bar) / beta_bar;
+    f[6] = (bvy * bz_bar - bvz * by_bar) * inv_bb;
     f[7] = ecoef * f[0] + (vx_bar * f[1] + vy_bar * f[2] + vz_bar * f[3]) +
            (bx_bar * f[4] + by_bar * f[5] + bz_bar * f[6]) - 0.5 * vy_bar * b_sq_bar + vb * by_bar;
   }
@@ -180,11 +193,13 @@ __device__ __forceinline__ void ec_flux(const double* a, const double* b, double
 
 // ESPP_HLL_flux_x (DG_solver.f90:894-1071).  wl, wr: conserved states already rotated into the
 // face normal frame (swap_xy for y faces).  out[0..7] = numerical flux, out[8] = nBn,
-// out[9] = sl, out[10] = sr.
+// out[9] = sl, out[10] = sr.  Quotients that share a denominator are formed as products with one
+// reciprocal (1/p, 1/(gamma-1), 1/(sqrt(rho_l)+sqrt(rho_r)), 1/a_form, 1/(sr-sl)); the values agree
+// with the reference's expression order to a few ulp.
 __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, double gamma, double* out) {
   const double rho_l = wl[0], mx_l = wl[1], my_l = wl[2], mz_l = wl[3], bx_l = wl[4], by_l = wl[5], bz_l = wl[6], e_l = wl[7];
   const double rho_r = wr[0], mx_r = wr[1], my_r = wr[2], mz_r = wr[3], bx_r = wr[4], by_r = wr[5], bz_r = wr[6], e_r = wr[7];
-  const double gm1 = gamma - 1.0;
+  const double gm1 = gamma - 1.0, igm1 = 1.0 / gm1;
   const double ir_l = 1.0 / rho_l, ir_r = 1.0 / rho_r;
   const double vx_l = ir_l * mx_l, vx_r = ir_r * mx_r;
   const double vy_l = ir_l * my_l, vy_r = ir_r * my_r;
@@ -196,6 +211,7 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
   const double pm_l = 0.5 * bsq_l, pm_r = 0.5 * bsq_r;
   const double p_l = fmax(gm1 * (e_l - (ek_l + pm_l)), PP_EPS);
   const double p_r = fmax(gm1 * (e_r - (ek_r + pm_r)), PP_EPS);
+  const double ip_l = 1.0 / p_l, ip_r = 1.0 / p_r;
   const double pt_l = p_l + pm_l, pt_r = p_r + pm_r;
   const double bu_l = bx_l * vx_l + by_l * vy_l + bz_l * vz_l;
   const double bu_r = bx_r * vx_r + by_r * vy_r + bz_r * vz_r;
@@ -203,12 +219,12 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
   const double ss_l = cs_l + bsq_l * ir_l, ss_r = cs_r + bsq_r * ir_r;
   const double cf_l = sqrt(0.5 * (ss_l + sqrt(fmax(ss_l * ss_l - 4.0 * cs_l * ir_l * (bx_l * bx_l), 0.0))));
   const double cf_r = sqrt(0.5 * (ss_r + sqrt(fmax(ss_r * ss_r - 4.0 * cs_r * ir_r * (bx_r * bx_r), 0.0))));
-  const double ith_l = rho_l / p_l, ith_r = rho_r / p_r;
+  const double ith_l = rho_l * ip_l, ith_r = rho_r * ip_r;
   const double phi_l = ith_l * bu_l, phi_r = ith_r * bu_r;
   const double se_l = log(p_l) - gamma * log(rho_l);
   const double se_r = log(p_r) - gamma * log(rho_r);
-  const double ef_l = (-rho_l * se_l / gm1) * vx_l;
-  const double ef_r = (-rho_r * se_r / gm1) * vx_r;
+  const double ef_l = (-rho_l * se_l * igm1) * vx_l;
+  const double ef_r = (-rho_r * se_r * igm1) * vx_r;
   double fl[8], fr[8], vl[8], vr[8];
   fl[0] = mx_l;
   fl[1] = vx_l * mx_l - bx_l * bx_l + pt_l;
@@ -226,26 +242,26 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
   fr[5] = -(bx_r * vy_r - by_r * vx_r);
   fr[6] = bz_r * vx_r - bx_r * vz_r;
   fr[7] = vx_r * (e_r + pt_r) - bx_r * bu_r;
-  vl[0] = (gamma - se_l) / gm1 - ek_l / p_l;
-  vl[1] = mx_l / p_l;
-  vl[2] = my_l / p_l;
-  vl[3] = mz_l / p_l;
+  vl[0] = (gamma - se_l) * igm1 - ek_l * ip_l;
+  vl[1] = mx_l * ip_l;
+  vl[2] = my_l * ip_l;
+  vl[3] = mz_l * ip_l;
   vl[4] = ith_l * bx_l;
   vl[5] = ith_l * by_l;
   vl[6] = ith_l * bz_l;
   vl[7] = -ith_l;
-  vr[0] = (gamma - se_r) / gm1 - ek_r / p_r;
-  vr[1] = mx_r / p_r;
-  vr[2] = my_r / p_r;
-  vr[3] = mz_r / p_r;
+  vr[0] = (gamma - se_r) * igm1 - ek_r * ip_r;
+  vr[1] = mx_r * ip_r;
+  vr[2] = my_r * ip_r;
+  vr[3] = mz_r * ip_r;
   vr[4] = ith_r * bx_r;
   vr[5] = ith_r * by_r;
   vr[6] = ith_r * bz_r;
   vr[7] = -ith_r;
   const double sq_l = sqrt(rho_l), sq_r = sqrt(rho_r);
-  const double sum_sq = sq_l + sq_r;
-  const double vx_roe = (vx_l * sq_l + vx_r * sq_r) / sum_sq;
-  const double db = sqrt((bx_l - bx_r) * (bx_l - bx_r) + (by_l - by_r) * (by_l - by_r) + (bz_l - bz_r) * (bz_l - bz_r)) / sum_sq;
+  const double isum = 1.0 / (sq_l + sq_r);
+  const double vx_roe = (vx_l * sq_l + vx_r * sq_r) * isum;
+  const double db = sqrt((bx_l - bx_r) * (bx_l - bx_r) + (by_l - by_r) * (by_l - by_r) + (bz_l - bz_r) * (bz_l - bz_r)) * isum;
   const double sl_pp = fmin(vx_l, vx_roe) - cf_l - db;
   const double sr_pp = fmax(vx_r, vx_roe) + cf_r + db;
   double da = 0.0, dbl = 0.0, dbr = 0.0;
@@ -256,16 +272,16 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
     dbl += vl[s] * dfs;
     dbr += vr[s] * dfs;
   }
-  const double a_form = fmax(da, 0.0) + 1e-8;
+  const double ia = 1.0 / (fmax(da, 0.0) + 1e-8);
   const double bl_form = (ef_r - ef_l) - dbl - phi_l * (bx_r - bx_l);
   const double br_form = (ef_r - ef_l) - dbr - phi_r * (bx_r - bx_l);
-  const double al = fmax(bl_form / a_form, 0.0);
-  const double ar = fmax(br_form / a_form, 0.0);
+  const double al = fmax(bl_form * ia, 0.0);
+  const double ar = fmax(br_form * ia, 0.0);
   const double aa = sqrt(al * ar);
   const double sl = fmin(fmin(-(ar + aa), sl_pp), 0.0);
   const double sr = fmax(fmax(al + aa, sr_pp), 0.0);
-  const double dslr = sr - sl;
-  const double wl_ = sr / dslr, wr_ = -sl / dslr, wd = (sl * sr) / dslr;
+  const double idsl = 1.0 / (sr - sl);
+  const double wl_ = sr * idsl, wr_ = -sl * idsl, wd = (sl * sr) * idsl;
 #pragma unroll
   for (int s = 0; s < 8; ++s) out[s] = wl_ * fl[s] + wr_ * fr[s] + wd * (wr[s] - wl[s]);
   out[8] = wl_ * bx_l + wr_ * bx_r;
