@@ -100,7 +100,7 @@ void member_work(const mhd_gpu* h, long long* cnt, InstDesc& d) {
   const long long nelg = (nx + 2) * (ny + 2);
   d.nblk_avg = (int)((nelg + TE - 1) / TE);
   cnt[WK_AVG] = d.nblk_avg;
-  cnt[WK_SIG] = (((nx + 1) * ny + nx * (ny + 1)) * 8 + 255) / 256;
+  cnt[WK_SIG] = ((nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX) * ((ny + SigCfg<P>::TY - 1) / SigCfg<P>::TY);
   d.nseg_limit = (int)(((nx + TE - 1) / TE) * ny);
   cnt[WK_LIM] = d.nseg_limit;
   cnt[WK_CMB] = (nx * ny * EB + 255) / 256;
@@ -228,7 +228,7 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
       pp_reduce_batched<<<b->nsm, 256, 0, st>>>(in, ninst, fin, ST_RUN);
       pp_sigsum_batched<P><<<grid_sig, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);
     }
-    pp_limit_batched<P><<<grid_lim, PP_NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
+    if (fin) pp_limit_batched<P><<<grid_lim, PP_NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
     if (fin) pp_entsum_batched<<<b->nsm, 256, 0, st>>>(in, ninst, ST_RUN);
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_END, R, s);
     bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);

@@ -201,16 +201,20 @@ void launch_combine(mhd_gpu* h, int stage, const double* dt_ptr, double dt, int 
 
 // post_process on slot `slot` (everything but the control-block reset and the host read-back)
 template <int P>
+// fuse = 1 (time-step pipeline only): a stage without OEDG, entropy or acceptance copy runs loops
+// 1 and 3 in one kernel (the stage result is discarded if an average is inadmissible)
 void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const double* dt_ptr, double oedg_dt,
-                 int ent_offset, int comput_ent, double* accept_dst, int gate) {
+                 int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0) {
   const int nb1 = pp_nblk_avg<P>(h);
+  const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
   pp_avg_ldf_kernel<P><<<nb1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
                                                       apply_oedg, ent_offset, h->partial, h->cell_ent_DG,
-                                                      h->cell_ent_FV, h->cell_ent_nan);
+                                                      h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1);
+  if (limit_in_loop1) return;
   if (apply_oedg) {
     pp_reduce_kernel<<<1, 256, 0, h->stream>>>(h->partial, nb1, h->ctrl, gate);
-    const long long nf = ((long long)(h->nx + 1) * h->ny + (long long)h->nx * (h->ny + 1)) * 8;
-    pp_sigsum_kernel<P><<<grid1d(nf, 256), 256, 0, h->stream>>>(h->u[slot], h->geo, h->ctrl, gate, h->sig_x, h->sig_y);
+    const dim3 gs((h->nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX, (h->ny + SigCfg<P>::TY - 1) / SigCfg<P>::TY);
+    pp_sigsum_kernel<P><<<gs, 256, 0, h->stream>>>(h->u[slot], h->geo, h->ctrl, gate, h->sig_x, h->sig_y);
   }
   dim3 g3 = pp_grid_limit<P>(h);
   pp_limit_kernel<P><<<g3, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_oedg, dt_ptr,
@@ -264,7 +268,7 @@ void enqueue_try(mhd_gpu* h) {
     launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
     launch_bc<P>(h, h->u[s], ST_RUN);
     launch_post<P>(h, s, h->use_oedg && fin, h->use_ldf, &h->ctrl->dt, 0.0, h->ent_offset, fin,
-                   fin ? h->u[0] : nullptr, ST_RUN);
+                   fin ? h->u[0] : nullptr, ST_RUN, 1);
     ctl_stage_end<<<1, 1, 0, h->stream>>>(h->ctrl);
     launch_bc<P>(h, h->u[s], ST_RUN);
     launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN);

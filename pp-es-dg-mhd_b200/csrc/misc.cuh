@@ -279,13 +279,13 @@ __device__ __forceinline__ void ctl_stage_time_body(Ctrl* c, int R, int s) {
 // otherwise account the limiter count and arm the dt_lim reduction of the coming residual.
 __device__ __forceinline__ void ctl_stage_end_body(Ctrl* c) {
   if (c->state != ST_RUN) return;
+  if (c->neg_avg) {  // checked first: a stage whose loops 1 and 3 ran fused may also hold a
+    c->state = ST_FAILED;  // re-limit failure that the reference, skipping loop 3, never reaches
+    return;
+  }
   if (c->pp_relimit) {
     c->flags |= 2;  // MHD_FLAG_PP_RELIMIT (the reference stops the program)
     c->state = ST_IDLE;
-    return;
-  }
-  if (c->neg_avg) {
-    c->state = ST_FAILED;
     return;
   }
   c->num_negcell_last = c->num_negcell;

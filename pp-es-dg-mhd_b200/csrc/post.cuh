@@ -173,6 +173,13 @@ __device__ __forceinline__ void limit_elements(double* s_u, const double* s_avg,
 // loop 1: averages + admissibility + LDF.  A CTA owns TE consecutive element blocks of the
 // ghosted grid (one contiguous run of memory).
 // ---------------------------------------------------------------------------------------------
+//
+// limit = 1 fuses loop 3 for a stage without OEDG and without the entropy sum: the interior
+// elements of the chunk are limited in shared memory before the one write-back.  The reference
+// skips loop 3 altogether when any element has an inadmissible average (neg_avg); here other CTAs
+// may already have limited their elements by then.  That is only allowed where the stage result
+// is discarded on neg_avg (the time-step pipeline re-tries the step from u_con), so the stand-alone
+// post_process never fuses.
 template <int P>
 __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg,
                                                  const Geo& g, Ctrl* ctrl, long long chunk, int apply_ldf,
@@ -180,7 +187,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
                                                  double* __restrict__ partial_out,  // 8 doubles
                                                  double* __restrict__ cell_ent_DG,
                                                  double* __restrict__ cell_ent_FV,
-                                                 unsigned char* __restrict__ cell_ent_nan) {
+                                                 unsigned char* __restrict__ cell_ent_nan, int limit = 0) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, TE = C::TE;
   __shared__ __align__(16) double s_u[TE * EB];
@@ -284,6 +291,9 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
     }
   }
   __syncthreads();
+  if (limit)  // loop 3 on the interior elements (DG_solver.f90:526-633)
+    limit_elements<P>(s_u, s_avg, s_inner, ne, e0, g, ctrl, ent_offset, 0, cell_ent_DG, cell_ent_FV, cell_ent_nan,
+                      nullptr);
 
   // write back state and averages
   for (int it = tid; it < ne * EB / 2; it += PP_NT) {
@@ -354,14 +364,15 @@ __global__ void __launch_bounds__(PP_NT)
                       int gate, int apply_ldf, int need_global, int ent_offset,
                       double* __restrict__ partial_sum,  // [gridDim.x][8]
                       double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
-                      unsigned char* __restrict__ cell_ent_nan) {
+                      unsigned char* __restrict__ cell_ent_nan, int limit) {
   if (!gate_open(ctrl, gate)) return;
   pp_avg_ldf_chunk<P>(u, u_avg, g, ctrl, blockIdx.x, apply_ldf, need_global, ent_offset,
-                      partial_sum + (long long)blockIdx.x * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan);
+                      partial_sum + (long long)blockIdx.x * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit);
 }
 
 // many instances: items = every member's chunks; slot = the stage state; `final` selects the
-// final-stage form (OEDG global reductions for instances that use OEDG)
+// final-stage form (OEDG global reductions for instances that use OEDG); the other stages fuse
+// loop 3 (limit)
 template <int P>
 __global__ void __launch_bounds__(PP_NT)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
@@ -373,7 +384,7 @@ __global__ void __launch_bounds__(PP_NT)
     if (!gate_open(d.ctrl, gate)) continue;
     pp_avg_ldf_chunk<P>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, d.use_oedg && final,
                         d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
-                        d.cell_ent_nan);
+                        d.cell_ent_nan, !final);
     __syncthreads();
   }
 }
@@ -424,161 +435,203 @@ __global__ void __launch_bounds__(256) pp_reduce_batched(const InstDesc* __restr
 }
 
 // ---------------------------------------------------------------------------------------------
-// OEDG face jump indicators.  One thread per (face, variable).  x faces first, then y faces.
+// OEDG face jump indicators (DG_solver.f90:295-422), one value per (face, variable):
 //   sigsum = sum_{kk,ll} (2m+1) h^m / (2 max(2p-1,1) kk! ll!) * <0.5 w, |d^kk_x d^ll_y jump|>
+// A CTA owns a TX x TY tile of interior elements and computes the left x face and the bottom y
+// face of each (plus the right/top boundary faces on the last tile of a row/column).  The tile
+// and its left/bottom neighbours (and the ghost column/row on the last tiles) are staged in
+// shared memory with coalesced loads; each (face, variable) item then reads two variable blocks.
+// Shared records are padded (NN+1 doubles per variable) against bank conflicts.
 // ---------------------------------------------------------------------------------------------
+// x face: L, R = the variable's nodes [k + N*l] of the left and right element
 template <int P>
-__device__ __forceinline__ void pp_sigsum_item(const double* __restrict__ u, const Geo& g, long long it,
-                                               double* __restrict__ sig_x, double* __restrict__ sig_y) {
-  constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
-  const int nx = g.nx, ny = g.ny, NXG = nx + 2;
-  const long long nfx = (long long)(nx + 1) * ny * 8;
-  const long long nfy = (long long)nx * (ny + 1) * 8;
-  if (it >= nfx + nfy) return;
+__device__ __forceinline__ double sigsum_x_face(const double* R, const double* Lf, double hx, double hy) {
+  constexpr int N = P + 1;
   const DegConst& dc = c_deg[P];
   const int denom_base = 2 * max(2 * P - 1, 1);
+  const double sx = 2.0 / hx, sy = 2.0 / hy;
   double total = 0.0;
-  if (it < nfx) {  // x face between (i-1,j) and (i,j), i = 1..nx+1, j = 1..ny (DG_solver.f90:296-343)
-    const int v = (int)(it & 7);
-    const long long f = it >> 3;
-    const int j = 1 + (int)(f / (nx + 1)), i = 1 + (int)(f - (long long)(j - 1) * (nx + 1));
-    const double* uR = u + ((long long)j * NXG + i) * EB + v * NN;
-    const double* uL = u + ((long long)j * NXG + i - 1) * EB + v * NN;
-    double R[NN], Lf[NN];
+  double sxk = 1.0, hx_pow_kk = 1.0;
+  int fac_kk = 1;
+#pragma unroll 1
+  for (int kk = 0; kk <= P; ++kk) {
+    double jump[N];
 #pragma unroll
-    for (int q = 0; q < NN; ++q) {
-      R[q] = __ldg(uR + q);
-      Lf[q] = __ldg(uL + q);
-    }
-    const double sx = 2.0 / g.hx, sy = 2.0 / g.hy, hx = g.hx;
-    double sxk = 1.0, hx_pow_kk = 1.0;
-    int fac_kk = 1;
-#pragma unroll
-    for (int kk = 0; kk <= P; ++kk) {
-      double jump[N];
-#pragma unroll
-      for (int l = 0; l < N; ++l) {
-        double tr = 0.0, tl = 0.0;
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-          tr += dc.R0[kk][k] * R[k + N * l];
-          tl += dc.RN[kk][k] * Lf[k + N * l];
-        }
-        jump[l] = sxk * tr - sxk * tl;
-      }
-      int fac_ll = 1;
-      double h_pow = hx_pow_kk;
-#pragma unroll
-      for (int ll = 0; ll <= P - kk; ++ll) {
-        double L1 = 0.0;
-#pragma unroll
-        for (int l = 0; l < N; ++l) L1 += (0.5 * dc.qw[l]) * fabs(jump[l]);
-        const double coef = ((2 * (kk + ll) + 1) * h_pow) / (double)(denom_base * fac_kk * fac_ll);
-        total = total + coef * L1;
-        if (ll < P) {
-          double nj[N];
-#pragma unroll
-          for (int a = 0; a < N; ++a) {
-            double s = 0.0;
-#pragma unroll
-            for (int b = 0; b < N; ++b) s += (sy * dc.D[a + N * b]) * jump[b];
-            nj[a] = s;
-          }
-#pragma unroll
-          for (int a = 0; a < N; ++a) jump[a] = nj[a];
-          fac_ll *= (ll + 1);
-          h_pow *= hx;
-        }
-      }
-      if (kk < P) {
-        fac_kk *= (kk + 1);
-        hx_pow_kk *= hx;
-        sxk *= sx;
-      }
-    }
-    sig_x[f * 8 + v] = total;
-  } else {  // y face between (i,j-1) and (i,j), i = 1..nx, j = 1..ny+1 (DG_solver.f90:360-407)
-    const long long it2 = it - nfx;
-    const int v = (int)(it2 & 7);
-    const long long f = it2 >> 3;
-    const int j = 1 + (int)(f / nx), i = 1 + (int)(f - (long long)(j - 1) * nx);
-    const double* uT = u + ((long long)j * NXG + i) * EB + v * NN;
-    const double* uB = u + ((long long)(j - 1) * NXG + i) * EB + v * NN;
-    double T[NN], B[NN];
-#pragma unroll
-    for (int q = 0; q < NN; ++q) {
-      T[q] = __ldg(uT + q);
-      B[q] = __ldg(uB + q);
-    }
-    const double sx = 2.0 / g.hx, sy = 2.0 / g.hy, hy = g.hy;
-    double syl = 1.0, hy_pow_ll = 1.0;
-    int fac_ll = 1;
-#pragma unroll
-    for (int ll = 0; ll <= P; ++ll) {
-      double jump[N];
+    for (int l = 0; l < N; ++l) {
+      double tr = 0.0, tl = 0.0;
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        double tt = 0.0, tb = 0.0;
-#pragma unroll
-        for (int l = 0; l < N; ++l) {
-          tt += dc.R0[ll][l] * T[k + N * l];
-          tb += dc.RN[ll][l] * B[k + N * l];
-        }
-        jump[k] = syl * tt - syl * tb;
+        tr += dc.R0[kk][k] * R[k + N * l];
+        tl += dc.RN[kk][k] * Lf[k + N * l];
       }
-      int fac_kk = 1;
-      double h_pow = hy_pow_ll;
+      jump[l] = sxk * tr - sxk * tl;
+    }
+    int fac_ll = 1;
+    double h_pow = hx_pow_kk;
 #pragma unroll
-      for (int kk = 0; kk <= P - ll; ++kk) {
-        double L1 = 0.0;
+    for (int ll = 0; ll <= P - kk; ++ll) {
+      double L1 = 0.0;
 #pragma unroll
-        for (int k = 0; k < N; ++k) L1 += (0.5 * dc.qw[k]) * fabs(jump[k]);
-        const double coef = ((2 * (kk + ll) + 1) * h_pow) / (double)(denom_base * fac_kk * fac_ll);
-        total = total + coef * L1;
-        if (kk < P) {
-          double nj[N];
-#pragma unroll
-          for (int a = 0; a < N; ++a) {
-            double s = 0.0;
-#pragma unroll
-            for (int b = 0; b < N; ++b) s += (sx * dc.D[a + N * b]) * jump[b];
-            nj[a] = s;
-          }
-#pragma unroll
-          for (int a = 0; a < N; ++a) jump[a] = nj[a];
-          fac_kk *= (kk + 1);
-          h_pow *= hy;
-        }
-      }
+      for (int l = 0; l < N; ++l) L1 += (0.5 * dc.qw[l]) * fabs(jump[l]);
+      const double coef = ((2 * (kk + ll) + 1) * h_pow) / (double)(denom_base * fac_kk * fac_ll);
+      total = total + coef * L1;
       if (ll < P) {
+        double nj[N];
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+          double acc = 0.0;
+#pragma unroll
+          for (int b = 0; b < N; ++b) acc += (sy * dc.D[a + N * b]) * jump[b];
+          nj[a] = acc;
+        }
+#pragma unroll
+        for (int a = 0; a < N; ++a) jump[a] = nj[a];
         fac_ll *= (ll + 1);
-        hy_pow_ll *= hy;
-        syl *= sy;
+        h_pow *= hx;
       }
     }
-    sig_y[f * 8 + v] = total;
+    if (kk < P) {
+      fac_kk *= (kk + 1);
+      hx_pow_kk *= hx;
+      sxk *= sx;
+    }
+  }
+  return total;
+}
+
+// y face: B, T = the variable's nodes of the bottom and top element
+template <int P>
+__device__ __forceinline__ double sigsum_y_face(const double* T, const double* B, double hx, double hy) {
+  constexpr int N = P + 1;
+  const DegConst& dc = c_deg[P];
+  const int denom_base = 2 * max(2 * P - 1, 1);
+  const double sx = 2.0 / hx, sy = 2.0 / hy;
+  double total = 0.0;
+  double syl = 1.0, hy_pow_ll = 1.0;
+  int fac_ll = 1;
+#pragma unroll 1
+  for (int ll = 0; ll <= P; ++ll) {
+    double jump[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double tt = 0.0, tb = 0.0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        tt += dc.R0[ll][l] * T[k + N * l];
+        tb += dc.RN[ll][l] * B[k + N * l];
+      }
+      jump[k] = syl * tt - syl * tb;
+    }
+    int fac_kk = 1;
+    double h_pow = hy_pow_ll;
+#pragma unroll
+    for (int kk = 0; kk <= P - ll; ++kk) {
+      double L1 = 0.0;
+#pragma unroll
+      for (int k = 0; k < N; ++k) L1 += (0.5 * dc.qw[k]) * fabs(jump[k]);
+      const double coef = ((2 * (kk + ll) + 1) * h_pow) / (double)(denom_base * fac_kk * fac_ll);
+      total = total + coef * L1;
+      if (kk < P) {
+        double nj[N];
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+          double acc = 0.0;
+#pragma unroll
+          for (int b = 0; b < N; ++b) acc += (sx * dc.D[a + N * b]) * jump[b];
+          nj[a] = acc;
+        }
+#pragma unroll
+        for (int a = 0; a < N; ++a) jump[a] = nj[a];
+        fac_kk *= (kk + 1);
+        h_pow *= hy;
+      }
+    }
+    if (ll < P) {
+      fac_ll *= (ll + 1);
+      hy_pow_ll *= hy;
+      syl *= sy;
+    }
+  }
+  return total;
+}
+
+template <int P>
+struct SigCfg;
+template <>
+struct SigCfg<1> { static constexpr int TX = 8, TY = 8; };
+template <>
+struct SigCfg<2> { static constexpr int TX = 8, TY = 4; };
+template <>
+struct SigCfg<3> { static constexpr int TX = 4, TY = 4; };
+
+template <int P>
+struct SigLayout {
+  static constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
+  static constexpr int TX = SigCfg<P>::TX, TY = SigCfg<P>::TY;
+  static constexpr int VS = NN + 1, ES = 8 * VS;   // padded variable / element record
+  static constexpr int RW = TX + 2, RH = TY + 2;   // staged rectangle (max)
+  static constexpr int DOUBLES = RW * RH * ES;
+};
+
+template <int P>
+__device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, int tile_x, int tile_y,
+                                               double* __restrict__ sig_x, double* __restrict__ sig_y) {
+  using L = SigLayout<P>;
+  constexpr int NN = L::NN, EB = L::EB, VS = L::VS, ES = L::ES, TX = L::TX, TY = L::TY, RW = L::RW;
+  constexpr int NT = 256;
+  __shared__ double s_e[L::DOUBLES];  // face math reads its two variable blocks from here
+  const int tid = threadIdx.x;
+  const int nx = g.nx, ny = g.ny, NXG = nx + 2;
+  const int i0 = 1 + tile_x * TX, j0 = 1 + tile_y * TY;
+  const int W = min(TX, nx - i0 + 1), H = min(TY, ny - j0 + 1);
+  const int right = (i0 + W - 1 == nx), top = (j0 + H - 1 == ny);
+  const int cw = W + 1 + right, rh = H + 1 + top;  // staged columns i0-1 .., rows j0-1 ..
+  // stage: rect row rr = grid row j0-1+rr, rect column cc = grid column i0-1+cc
+  for (int it = tid; it < rh * cw * EB; it += NT) {
+    const int rr = it / (cw * EB), rem = it - rr * cw * EB;  // rem indexes a contiguous run of cw elements
+    const int cc = rem / EB, w = rem - cc * EB, v = w / NN, q = w - v * NN;
+    s_e[(rr * RW + cc) * ES + v * VS + q] = __ldg(u + ((long long)(j0 - 1 + rr) * NXG + (i0 - 1)) * EB + rem);
+  }
+  __syncthreads();
+  const int nfx = H * (W + right), nfy = W * (H + top);
+  for (int it = tid; it < 8 * (nfx + nfy); it += NT) {
+    const int v = it & 7, f = it >> 3;
+    if (f < nfx) {  // x face: row r, face c between columns c-1 and c of the tile
+      const int r = f / (W + right), c = f - r * (W + right);
+      const double* pl = s_e + ((r + 1) * RW + c) * ES + v * VS;
+      const int i = i0 + c, j = j0 + r;
+      sig_x[(((long long)(j - 1) * (nx + 1)) + (i - 1)) * 8 + v] = sigsum_x_face<P>(pl + ES, pl, g.hx, g.hy);
+    } else {  // y face: column c, face r between rows r-1 and r of the tile
+      const int f2 = f - nfx;
+      const int c = f2 / (H + top), r = f2 - c * (H + top);
+      const double* pb = s_e + (r * RW + c + 1) * ES + v * VS;
+      const int i = i0 + c, j = j0 + r;
+      sig_y[(((long long)(j - 1) * nx) + (i - 1)) * 8 + v] = sigsum_y_face<P>(pb + RW * ES, pb, g.hx, g.hy);
+    }
   }
 }
 
 template <int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
                      double* __restrict__ sig_x, double* __restrict__ sig_y) {
   if (!gate_open(ctrl, gate)) return;
-  pp_sigsum_item<P>(u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x, sig_x, sig_y);
+  pp_sigsum_tile<P>(u, g, blockIdx.x, blockIdx.y, sig_x, sig_y);
 }
 
-// many instances: items = every member's blocks of 256 (face, variable) pairs
+// many instances: items = every member's tiles (row-major)
 template <int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     pp_sigsum_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   const int nw = *nwork, n = *ninst;
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+    const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
-    pp_sigsum_item<P>(d.u[slot], d.g, (long long)chunk * 256 + threadIdx.x, d.sig_x, d.sig_y);
+    const int ntx = (d.g.nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX;
+    pp_sigsum_tile<P>(d.u[slot], d.g, local % ntx, local / ntx, d.sig_x, d.sig_y);
+    __syncthreads();  // the next tile reuses shared memory
   }
 }
 
