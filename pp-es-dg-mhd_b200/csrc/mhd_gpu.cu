@@ -7,6 +7,7 @@
 // single-thread control kernels on the device, so the host only polls a status block.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -112,6 +113,20 @@ int pp_nblk_avg(const mhd_gpu* h) { return grid1d((long long)(h->nx + 2) * (h->n
 template <int P>
 dim3 pp_grid_limit(const mhd_gpu* h) { return dim3((h->nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE, h->ny); }
 
+// CTAs of pp_avg_ldf_kernel<P> the device holds at once (its grid walks the chunks)
+template <int P>
+int pp_resident_ctas(int dev) {
+  static int cached[kMaxDevices];
+  if (dev < 0 || dev >= kMaxDevices) return 1;
+  if (!cached[dev]) {
+    int nsm = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pp_avg_ldf_kernel<P>, PP_NT, 0);
+    cached[dev] = std::max(1, nsm) * std::max(1, per_sm);
+  }
+  return cached[dev];
+}
+
 int init_device_tables(int dev) {
   std::lock_guard<std::mutex> lk(g_init_mutex);
   if (dev < 0 || dev >= kMaxDevices) return MHD_ERR_INVALID;
@@ -207,9 +222,10 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
                  int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0) {
   const int nb1 = pp_nblk_avg<P>(h);
   const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
-  pp_avg_ldf_kernel<P><<<nb1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
-                                                      apply_oedg, ent_offset, h->partial, h->cell_ent_DG,
-                                                      h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1);
+  const int grid1 = std::min(nb1, pp_resident_ctas<P>(h->device));
+  pp_avg_ldf_kernel<P><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
+                                                        apply_oedg, ent_offset, h->partial, h->cell_ent_DG,
+                                                        h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
   if (limit_in_loop1) return;
   if (apply_oedg) {
     pp_reduce_kernel<<<1, 256, 0, h->stream>>>(h->partial, nb1, h->ctrl, gate);

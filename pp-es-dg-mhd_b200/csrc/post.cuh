@@ -2,372 +2,308 @@
 //
 //   pp_avg_ldf_kernel   loop 1 (DG_solver.f90:161-277): cell averages of every interior and
 //                       non-corner ghost element, admissibility of the average, the LDF projection
-//                       of (Bx,By) as one dense nodal operator, and (for OEDG) per-block partial
-//                       sums of the average plus max/min of the post-LDF interior values.
+//                       of (Bx,By) as one dense nodal operator, and (for OEDG) per-chunk partial
+//                       sums of the average plus max/min of the post-LDF interior values.  In the
+//                       time-step pipeline a stage without OEDG also runs loop 3 here (fused).
 //   pp_reduce_kernel    the global average sum (fixed order) and u_vari_global (DG_solver.f90:282-294):
 //                       max|u - g| = max(umax - g, g - umin) because rounding is monotone.
 //   pp_sigsum_kernel    the OEDG face jump indicators OEDG_sigsum_x/y (DG_solver.f90:295-422).
 //   pp_limit_kernel     loop 3 (DG_solver.f90:428-656): OEDG damping, Zhang-Shu positivity
 //                       scaling with its bounded re-limit loop, entropy-offset limiting, cell
-//                       entropy (block partials, fixed order).
+//                       entropy (chunk partials, fixed order).
 //   pp_entsum_kernel    total entropy from the partials (fixed order).
+//
+// Loops 1 and 3 work element-locally, so they map one element to a group of GS lanes of a warp,
+// one lane per GLL node, each lane holding its node's 8 variables in registers.  Loads and stores
+// of a variable are then 8*NN-byte runs per group (coalesced), per-element sums, minima and maxima
+// are butterfly reductions inside the group (every lane ends with the same value, since IEEE
+// addition, min and max are commutative), and no CTA-wide barrier sits between the steps of one
+// element.  A CTA of PP_NT threads handles a chunk of TE = (PP_NT/32) * (32/GS) consecutive
+// elements; per-chunk partial sums are formed in element order.
 #pragma once
 #include "common.cuh"
 
 namespace mhd {
 
 constexpr int PP_NT = 256;
+constexpr unsigned FULL_MASK = 0xffffffffu;
 
 template <int P>
 struct PPCfg {
   static constexpr int N = P + 1, NN = N * N, EB = 8 * NN, N2 = 2 * NN;
-  static constexpr int TE = (P == 1) ? 64 : (P == 2 ? 32 : 16);  // elements per CTA
+  static constexpr int GS = NN <= 4 ? 4 : (NN <= 8 ? 8 : (NN <= 16 ? 16 : 32));  // lanes per element
+  static constexpr int G = 32 / GS;                                               // elements per warp
+  static constexpr int TE = (PP_NT / 32) * G;                                     // elements per CTA chunk
 };
 
-// ---------------------------------------------------------------------------------------------
-// Zhang-Shu positivity (DG_solver.f90:528-603), entropy-offset limiting (:606-633) and the cell
-// entropy (:635-649) of the elements a CTA holds in shared memory (s_u [e][var][node], s_avg
-// [e][8]).  Node-parallel: node pressures and entropies take one thread per node; the per-element
-// decisions take one lane per element; the rare re-limit loop stays serial per element.
-// mask (may be NULL = all) selects the elements to limit; cell-entropy arrays are indexed from
-// ebase; the CTA's entropy partial (elements in order) goes to *ent_out.
-// ---------------------------------------------------------------------------------------------
-template <int P>
-__device__ __forceinline__ void limit_elements(double* s_u, const double* s_avg, const unsigned char* mask, int ne,
-                                               long long ebase, const Geo& g, Ctrl* ctrl, int ent_offset,
-                                               int comput_ent, const double* __restrict__ cell_ent_DG,
-                                               const double* __restrict__ cell_ent_FV,
-                                               const unsigned char* __restrict__ cell_ent_nan,
-                                               double* __restrict__ ent_out) {
-  using C = PPCfg<P>;
-  constexpr int N = C::N, NN = C::NN, EB = C::EB, TE = C::TE;
-  constexpr double BIG = 1.7976931348623157e308;
-  __shared__ double l_nd[TE * NN];
-  __shared__ double l_thd[TE], l_thp[TE];
-  __shared__ int l_cnt;
-  const int tid = threadIdx.x;
-  const double gamma = g.gamma;
-  const DegConst& dc = c_deg[P];
-  if (tid == 0) l_cnt = 0;
-  // density: theta from the minimum nodal density (DG_solver.f90:538-553)
-  if (tid < ne) {
-    double th = -1.0;
-    if (!mask || mask[tid]) {
-      const double* x = s_u + tid * EB;
-      double den_min = BIG;
-      for (int q = 0; q < NN; ++q) den_min = fmin(den_min, x[q]);
-      if (den_min < PP_EPS) {
-        const double da = s_avg[tid * 8];
-        th = fmax(fmin((da - PP_EPS) / (da - den_min), 1.0), 0.0);
-      }
-    }
-    l_thd[tid] = th;
-  }
-  __syncthreads();
-  for (int it = tid; it < ne * NN; it += PP_NT) {
-    const int e = it / NN, q = it - e * NN;
-    const double th = l_thd[e];
-    if (th >= 0.0) {
-      const double a0 = s_avg[e * 8];
-      double x = s_u[e * EB + q];
-      x = a0 + th * (x - a0);
-      s_u[e * EB + q] = fmax(x, PP_EPS);
-    }
-  }
-  __syncthreads();
-  // pressure: nodal pressures in parallel, theta from their minimum (DG_solver.f90:556-571)
-  for (int it = tid; it < ne * NN; it += PP_NT) {
-    const int e = it / NN, q = it - e * NN;
-    if (mask && !mask[e]) continue;
-    const double* x = s_u + e * EB + q;
-    l_nd[it] = prs_of(x[0], x[NN], x[2 * NN], x[3 * NN], x[4 * NN], x[5 * NN], x[6 * NN], x[7 * NN], gamma);
-  }
-  __syncthreads();
-  if (tid < ne) {
-    double th = -1.0;
-    if (!mask || mask[tid]) {
-      double pmin = BIG;
-      for (int q = 0; q < NN; ++q) pmin = fmin(pmin, l_nd[tid * NN + q]);
-      if (pmin < PP_EPS) {
-        const double* a = s_avg + tid * 8;
-        const double pa = prs_of(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], gamma);
-        th = fmax(fmin((pa - PP_EPS) / (pa - pmin), 1.0), 0.0);
-      }
-      if (l_thd[tid] >= 0.0 || th >= 0.0) atomicAdd(&l_cnt, 1);  // neg_node (DG_solver.f90:602)
-    }
-    l_thp[tid] = th;
-  }
-  __syncthreads();
-  for (int it = tid; it < ne * EB; it += PP_NT) {
-    const int e = it / EB;
-    const double th = l_thp[e];
-    if (th >= 0.0) {
-      const double a = s_avg[e * 8 + (it - e * EB) / NN];
-      s_u[it] = a + th * (s_u[it] - a);
-    }
-  }
-  __syncthreads();
-  if (tid < ne) {
-    double* x = s_u + tid * EB;
-    const double* a = s_avg + tid * 8;
-    double theta = l_thp[tid];
-    if (theta >= 0.0) {  // re-check after the FP-inexact theta (DG_solver.f90:573-599), rare
-      for (int it_count = 0;; ++it_count) {  // bounded: at most two extra shrinks
-        double prs_min = BIG;
-        for (int q = 0; q < NN; ++q)
-          prs_min = fmin(prs_min, prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma));
-        if (!(prs_min < 0.99 * PP_EPS)) break;
-        if (it_count > 1) {
-          atomicOr(&ctrl->pp_relimit, 1);
-          break;
-        }
-        theta = 0.6 * theta;
-        for (int v = 0; v < 8; ++v)
-          for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + theta * (x[v * NN + q] - a[v]);
-      }
-    }
-    const long long ce = ebase + tid;
-    if (ent_offset && (!mask || mask[tid]) && !cell_ent_nan[ce]) {  // DG_solver.f90:606-633
-      const double old = cell_ent_DG[ce], eavg = cell_ent_FV[ce];
-      double nw = 0.0;
-      for (int l = 0; l < N; ++l)
-        for (int k = 0; k < N; ++k) {
-          const int q = k + N * l;
-          const double pq = fmax(prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], gamma), PP_EPS);
-          nw = nw + (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[q], pq, gamma);
-        }
-      if (nw > old) {
-        const double th = fmax(fmin((old - eavg) / (nw - eavg), 1.0), 0.0);
-        for (int v = 0; v < 8; ++v)
-          for (int q = 0; q < NN; ++q) x[v * NN + q] = a[v] + th * (x[v * NN + q] - a[v]);
-      }
-    }
-  }
-  __syncthreads();
-  if (comput_ent) {  // DG_solver.f90:635-649
-    for (int it = tid; it < ne * NN; it += PP_NT) {
-      const int e = it / NN, q = it - e * NN;
-      if (mask && !mask[e]) continue;
-      const int k = q % N, l = q / N;
-      const double* x = s_u + e * EB + q;
-      const double pq = fmax(prs_of(x[0], x[NN], x[2 * NN], x[3 * NN], x[4 * NN], x[5 * NN], x[6 * NN], x[7 * NN], gamma), PP_EPS);
-      l_nd[it] = (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[0], pq, gamma);
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double tot = 0.0;
-      for (int e = 0; e < ne; ++e) {
-        if (mask && !mask[e]) continue;
-        double ce = 0.0;
-        for (int q = 0; q < NN; ++q) ce = ce + l_nd[e * NN + q];
-        tot = tot + ce;
-      }
-      *ent_out = tot;
-    }
-  }
-  __syncthreads();
-  if (tid == 0 && l_cnt) atomicAdd(&ctrl->num_negcell, l_cnt);
+template <int GS>
+__device__ __forceinline__ double grp_sum(double v) {
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) v = v + __shfl_xor_sync(FULL_MASK, v, o);
+  return v;
+}
+template <int GS>
+__device__ __forceinline__ double grp_min(double v) {
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL_MASK, v, o));
+  return v;
+}
+template <int GS>
+__device__ __forceinline__ double grp_max(double v) {
+#pragma unroll
+  for (int o = GS / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double node_prs(const double* x, double gamma) {
+  return prs_of(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], gamma);
 }
 
 // ---------------------------------------------------------------------------------------------
-// loop 1: averages + admissibility + LDF.  A CTA owns TE consecutive element blocks of the
-// ghosted grid (one contiguous run of memory).
+// Loop 3 for the element of this lane's group (DG_solver.f90:526-649): Zhang-Shu positivity with
+// its bounded re-limit loop, entropy-offset limiting, and the cell entropy.  x = this lane's node,
+// avg = the element average (all lanes of the group), node = lane's node (active = node < NN and
+// the group's element is limited).  Every lane of the warp calls this (the group reductions need
+// the whole warp); returns the cell entropy (0 where not computed) and sets *negcell.
 // ---------------------------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ double limit_group(double* x, const double* avg, bool active, bool lead, int node,
+                                              long long ce, const Geo& g, Ctrl* ctrl, int ent_offset,
+                                              int comput_ent, const double* __restrict__ cell_ent_DG,
+                                              const double* __restrict__ cell_ent_FV,
+                                              const unsigned char* __restrict__ cell_ent_nan, bool* negcell) {
+  using C = PPCfg<P>;
+  constexpr int N = C::N, GS = C::GS;
+  constexpr double BIG = 1.7976931348623157e308;
+  const double gamma = g.gamma;
+  const DegConst& dc = c_deg[P];
+  // density: theta from the minimum nodal density (DG_solver.f90:538-553)
+  const double den_min = grp_min<GS>(active ? x[0] : BIG);
+  double thd = -1.0;
+  if (den_min < PP_EPS) thd = fmax(fmin((avg[0] - PP_EPS) / (avg[0] - den_min), 1.0), 0.0);
+  if (active && thd >= 0.0) x[0] = fmax(avg[0] + thd * (x[0] - avg[0]), PP_EPS);
+  // pressure: theta from the minimum nodal pressure (DG_solver.f90:556-571)
+  const double pmin = grp_min<GS>(active ? node_prs(x, gamma) : BIG);
+  double thp = -1.0;
+  if (pmin < PP_EPS) {
+    const double pa = prs_of(avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6], avg[7], gamma);
+    thp = fmax(fmin((pa - PP_EPS) / (pa - pmin), 1.0), 0.0);
+  }
+  *negcell = lead && active && (thd >= 0.0 || thp >= 0.0);  // neg_node (DG_solver.f90:602)
+  if (active && thp >= 0.0)
+#pragma unroll
+    for (int v = 0; v < 8; ++v) x[v] = avg[v] + thp * (x[v] - avg[v]);
+  // re-check after the FP-inexact theta (DG_solver.f90:573-599): at most two extra shrinks; the
+  // loop runs while any group of the warp still checks, so that the reductions see the whole warp
+  bool pending = active && thp >= 0.0;
+  double theta = thp;
+  for (int it_count = 0; __any_sync(FULL_MASK, pending); ++it_count) {
+    const double pm = grp_min<GS>(pending ? node_prs(x, gamma) : BIG);
+    if (pending) {
+      if (!(pm < 0.99 * PP_EPS)) {
+        pending = false;
+      } else if (it_count > 1) {
+        if (lead) atomicOr(&ctrl->pp_relimit, 1);
+        pending = false;
+      } else {
+        theta = 0.6 * theta;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) x[v] = avg[v] + theta * (x[v] - avg[v]);
+      }
+    }
+  }
+  const int k = node % N, l = node / N;
+  const double wq = (node < C::NN) ? 0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l] : 0.0;
+  // entropy-offset limiter (DG_solver.f90:606-633)
+  if (ent_offset) {
+    const bool use = active && !cell_ent_nan[ce];
+    const double nw = grp_sum<GS>(use ? wq * ent_of(x[0], fmax(node_prs(x, gamma), PP_EPS), gamma) : 0.0);
+    if (use) {
+      const double old = cell_ent_DG[ce], eavg = cell_ent_FV[ce];
+      if (nw > old) {
+        const double th = fmax(fmin((old - eavg) / (nw - eavg), 1.0), 0.0);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) x[v] = avg[v] + th * (x[v] - avg[v]);
+      }
+    }
+  }
+  // cell entropy (DG_solver.f90:635-649)
+  if (comput_ent) return grp_sum<GS>(active ? wq * ent_of(x[0], fmax(node_prs(x, gamma), PP_EPS), gamma) : 0.0);
+  return 0.0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// loop 1 for one chunk of TE consecutive element blocks of the ghosted grid (one contiguous run of
+// memory).  s_A = the LDF operator in shared memory; s_red = CTA scratch (TE * 8 + 128 doubles).
 //
 // limit = 1 fuses loop 3 for a stage without OEDG and without the entropy sum: the interior
-// elements of the chunk are limited in shared memory before the one write-back.  The reference
-// skips loop 3 altogether when any element has an inadmissible average (neg_avg); here other CTAs
-// may already have limited their elements by then.  That is only allowed where the stage result
-// is discarded on neg_avg (the time-step pipeline re-tries the step from u_con), so the stand-alone
+// elements are limited in registers before the one write-back.  The reference skips loop 3
+// altogether when any element has an inadmissible average (neg_avg); here other CTAs may already
+// have limited their elements by then.  That is only allowed where the stage result is discarded
+// on neg_avg (the time-step pipeline re-tries the step from u_con), so the stand-alone
 // post_process never fuses.
+// ---------------------------------------------------------------------------------------------
 template <int P>
-__device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg,
-                                                 const Geo& g, Ctrl* ctrl, long long chunk, int apply_ldf,
-                                                 int need_global, int ent_offset,
-                                                 double* __restrict__ partial_out,  // 8 doubles
-                                                 double* __restrict__ cell_ent_DG,
-                                                 double* __restrict__ cell_ent_FV,
-                                                 unsigned char* __restrict__ cell_ent_nan, int limit = 0) {
+__device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg, const Geo& g,
+                                                 Ctrl* ctrl, long long chunk, int apply_ldf, int need_global,
+                                                 int ent_offset, double* __restrict__ partial_out,  // 8 doubles
+                                                 double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
+                                                 unsigned char* __restrict__ cell_ent_nan, int limit,
+                                                 const double* s_A, double* s_red, int* s_cnt) {
   using C = PPCfg<P>;
-  constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, TE = C::TE;
-  __shared__ __align__(16) double s_u[TE * EB];
-  __shared__ double s_out[TE * N2];
-  __shared__ double s_avg[TE * 8];
-  __shared__ double s_A[N2 * N2];
-  __shared__ unsigned char s_valid[TE], s_inner[TE];
-  __shared__ double s_mx[8 * (PP_NT / 32)], s_mn[8 * (PP_NT / 32)];
-  const int tid = threadIdx.x;
+  constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = lane / GS, node = lane - grp * GS, gbase = grp * GS;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long total = (long long)NXG * (ny + 2);
   const long long e0 = chunk * TE;
   const int ne = (int)min((long long)TE, total - e0);
+  const int el = warp * G + grp;  // element of this group within the chunk
+  const long long e = e0 + el;
   const DegConst& dc = c_deg[P];
-
-  for (int it = tid; it < ne * EB / 2; it += PP_NT)
-    reinterpret_cast<double2*>(s_u)[it] = reinterpret_cast<const double2*>(u + e0 * EB)[it];
-  if (apply_ldf)
-    for (int it = tid; it < N2 * N2; it += PP_NT) s_A[it] = __ldg(g.ldfA + it);
-  if (tid < TE) {
-    const long long e = e0 + tid;
-    int valid = 0, inner = 0;
-    if (tid < ne) {
-      const int j = (int)(e / NXG), i = (int)(e - (long long)j * NXG);
-      const bool ii = (i >= 1 && i <= nx), jj = (j >= 1 && j <= ny);
-      valid = ii || jj;  // DG_solver.f90:165 (corners are skipped)
-      inner = ii && jj;
-    }
-    s_valid[tid] = (unsigned char)valid;
-    s_inner[tid] = (unsigned char)inner;
+  const double gamma = g.gamma;
+  bool valid = false, inner = false;
+  if (el < ne) {
+    const int j = (int)(e / NXG), i = (int)(e - (long long)j * NXG);
+    const bool ii = (i >= 1 && i <= nx), jj = (j >= 1 && j <= ny);
+    valid = ii || jj;  // DG_solver.f90:165 (corners are skipped)
+    inner = ii && jj;
   }
-  __syncthreads();
-
-  // cell averages: ua(s) += (0.25*qw_x(k)*qw_y(l)) * u(s,k,l), l outer, k inner (DG_solver.f90:177-184)
-  for (int it = tid; it < TE * 8; it += PP_NT) {
-    const int e = it >> 3, v = it & 7;
-    if (!s_valid[e]) continue;
-    const double* x = s_u + e * EB + v * NN;
-    double a = 0.0;
+  const bool nd = node < NN;
+  const bool act = valid && nd;
+  double x[8];
 #pragma unroll
-    for (int l = 0; l < N; ++l)
+  for (int v = 0; v < 8; ++v) x[v] = act ? u[e * EB + v * NN + node] : 0.0;
+  // cell averages (DG_solver.f90:177-184)
+  const int k = node % N, l = node / N;
+  const double w = nd ? 0.25 * dc.qw[k] * dc.qw[l] : 0.0;
+  double avg[8];
 #pragma unroll
-      for (int k = 0; k < N; ++k) a = a + (0.25 * dc.qw[k] * dc.qw[l]) * x[k + N * l];
-    s_avg[it] = a;
-  }
-  __syncthreads();
-
-  // admissibility of the average; cell entropy for the entropy-offset limiter (DG_solver.f90:186-224)
-  if (tid < TE && s_valid[tid]) {
-    const double* a = s_avg + tid * 8;
-    const double den = a[0];
-    const double prs = prs_of(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], g.gamma);
-    if (den < PP_EPS || prs < PP_EPS) {
-      // inadmissible average: the reference leaves this element unwritten (DG_solver.f90:189-193)
-      atomicOr(&ctrl->neg_avg, 1);
-      s_valid[tid] = 0;
-      s_inner[tid] = 0;
-    }
-    if (ent_offset) {
-      const long long e = e0 + tid;
-      const double* x = s_u + tid * EB;
-      bool flag = true;
-      double ce = 0.0;
-      for (int q = 0; q < NN; ++q) {
-        const double pq = prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], g.gamma);
-        flag = flag && (x[q] >= PP_EPS) && (pq >= PP_EPS);
-      }
-      if (flag) {
-        for (int l = 0; l < N; ++l)
-          for (int k = 0; k < N; ++k) {
-            const int q = k + N * l;
-            const double pq = prs_of(x[q], x[NN + q], x[2 * NN + q], x[3 * NN + q], x[4 * NN + q], x[5 * NN + q], x[6 * NN + q], x[7 * NN + q], g.gamma);
-            ce = ce + (0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l]) * ent_of(x[q], pq, g.gamma);
-          }
-      }
-      cell_ent_FV[e] = (den >= PP_EPS && prs >= PP_EPS) ? ent_of(den, prs, g.gamma) : 0.0;
-      cell_ent_DG[e] = flag ? ce : 0.0;
-      cell_ent_nan[e] = flag ? 0 : 1;
+  for (int v = 0; v < 8; ++v) avg[v] = grp_sum<GS>(w * x[v]);
+  // admissibility of the average (DG_solver.f90:186-193): an inadmissible element is left unwritten
+  if (valid) {
+    const double prs = prs_of(avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6], avg[7], gamma);
+    if (avg[0] < PP_EPS || prs < PP_EPS) {
+      if (node == 0) atomicOr(&ctrl->neg_avg, 1);
+      valid = inner = false;
     }
   }
-
-  __syncthreads();
-
-  // LDF projection of (Bx - avg, By - avg) with the dense nodal operator
+  // cell entropies for the entropy-offset limiter (DG_solver.f90:195-224)
+  if (ent_offset) {
+    const double pq = act ? node_prs(x, gamma) : 0.0;
+    const bool okq = !act || (x[0] >= PP_EPS && pq >= PP_EPS);
+    const double okall = grp_min<GS>(okq ? 1.0 : 0.0);
+    const double ce = grp_sum<GS>((act && okall > 0.5) ? 0.25 * g.hx * g.hy * dc.qw[k] * dc.qw[l] * ent_of(x[0], pq, gamma) : 0.0);
+    if (valid && node == 0) {
+      const double prs = prs_of(avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6], avg[7], gamma);
+      cell_ent_FV[e] = ent_of(avg[0], prs, gamma);
+      cell_ent_DG[e] = okall > 0.5 ? ce : 0.0;
+      cell_ent_nan[e] = okall > 0.5 ? 0 : 1;
+    }
+  }
+  // LDF projection of (Bx - avg, By - avg) with the dense nodal operator: this lane forms the
+  // outputs at its node (rows `node` and NN + node); the inputs come from the group's lanes
   if (apply_ldf) {
-    for (int it = tid; it < TE * N2; it += PP_NT) {
-      const int e = it / N2, o = it - e * N2;
-      if (!s_valid[e]) continue;
-      const double* xb = s_u + e * EB + 4 * NN;  // Bx then By, contiguous (vars 4 and 5)
-      const double ax = s_avg[e * 8 + 4], ay = s_avg[e * 8 + 5];
-      double acc = 0.0;
-#pragma unroll 8
-      for (int m = 0; m < N2; ++m) acc += s_A[o + N2 * m] * (xb[m] - (m < NN ? ax : ay));
-      s_out[it] = acc + (o < NN ? ax : ay);
-    }
-    __syncthreads();
-    for (int it = tid; it < TE * N2; it += PP_NT) {
-      const int e = it / N2, o = it - e * N2;
-      if (!s_valid[e]) continue;
-      s_u[e * EB + 4 * NN + o] = s_out[it];
-    }
-  }
-  __syncthreads();
-  if (limit)  // loop 3 on the interior elements (DG_solver.f90:526-633)
-    limit_elements<P>(s_u, s_avg, s_inner, ne, e0, g, ctrl, ent_offset, 0, cell_ent_DG, cell_ent_FV, cell_ent_nan,
-                      nullptr);
-
-  // write back state and averages
-  for (int it = tid; it < ne * EB / 2; it += PP_NT) {
-    const int e = (2 * it) / EB;
-    if (!s_valid[e]) continue;
-    reinterpret_cast<double2*>(u + e0 * EB)[it] = reinterpret_cast<const double2*>(s_u)[it];
-  }
-  for (int it = tid; it < ne * 8; it += PP_NT) {
-    if (!s_valid[it >> 3]) continue;
-    u_avg[e0 * 8 + it] = s_avg[it];
-  }
-
-  if (need_global) {
-    // per-block sum of (hx*hy)*avg over interior elements in element order (DG_solver.f90:227-229)
-    if (tid < 8) {
-      double sacc = 0.0;
-      for (int e = 0; e < ne; ++e)
-        if (s_inner[e]) sacc = sacc + (g.hx * g.hy) * s_avg[e * 8 + tid];
-      partial_out[tid] = sacc;
-    }
-    // per-variable max and min of the post-LDF interior node values
-    double vmax[8], vmin[8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      vmax[v] = -1.0e308;
-      vmin[v] = 1.0e308;
-    }
-    for (int it = tid; it < ne * NN; it += PP_NT) {
-      const int e = it / NN, q = it - e * NN;
-      if (!s_inner[e]) continue;
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        const double x = s_u[e * EB + v * NN + q];
-        vmax[v] = fmax(vmax[v], x);
-        vmin[v] = fmin(vmin[v], x);
+    double ox = 0.0, oy = 0.0;
+#pragma unroll 4
+    for (int m = 0; m < NN; ++m) {
+      const double bxm = __shfl_sync(FULL_MASK, x[4], gbase + m) - avg[4];
+      const double bym = __shfl_sync(FULL_MASK, x[5], gbase + m) - avg[5];
+      if (nd) {
+        ox += s_A[node + N2 * m] * bxm;
+        oy += s_A[NN + node + N2 * m] * bxm;
+        ox += s_A[node + N2 * (NN + m)] * bym;
+        oy += s_A[NN + node + N2 * (NN + m)] * bym;
       }
     }
+    if (valid) {
+      x[4] = ox + avg[4];
+      x[5] = oy + avg[5];
+    }
+  }
+  if (need_global) {
+    // chunk sum of (hx*hy)*avg over interior elements in element order (DG_solver.f90:227-229)
+    if (el < TE)
+#pragma unroll
+      for (int v = 0; v < 8; ++v)
+        if (v % GS == node) s_red[el * 8 + v] = inner ? (g.hx * g.hy) * avg[v] : 0.0;
+    // max and min of the post-LDF interior node values
+    const bool use = inner && nd;
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
+      double mx = use ? x[v] : -1.0e308, mn = use ? x[v] : 1.0e308;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
-        vmax[v] = fmax(vmax[v], __shfl_xor_sync(0xffffffffu, vmax[v], o));
-        vmin[v] = fmin(vmin[v], __shfl_xor_sync(0xffffffffu, vmin[v], o));
+        mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+        mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+      }
+      if (lane == 0) {
+        s_red[TE * 8 + v * 8 + warp] = mx;
+        s_red[TE * 8 + 64 + v * 8 + warp] = mn;
       }
     }
-    if ((tid & 31) == 0)
+  }
+  bool neg = false;
+  if (limit) {
+    __syncwarp();  // the group's lane 0 wrote the cell entropies limit_group reads
+    limit_group<P>(x, avg, inner && nd, inner && node == 0, node, e, g, ctrl, ent_offset, 0, cell_ent_DG, cell_ent_FV,
+                   cell_ent_nan, &neg);
+    const unsigned cnt = __popc(__ballot_sync(FULL_MASK, neg));
+    if (lane == 0 && cnt) atomicAdd(s_cnt, (int)cnt);
+  }
+  // write back state and averages of the admissible elements
+  if (valid && nd)
 #pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        s_mx[v * (PP_NT / 32) + (tid >> 5)] = vmax[v];
-        s_mn[v * (PP_NT / 32) + (tid >> 5)] = vmin[v];
-      }
+    for (int v = 0; v < 8; ++v) u[e * EB + v * NN + node] = x[v];
+  if (valid)
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (v % GS == node) u_avg[e * 8 + v] = avg[v];
+  if (need_global) {
     __syncthreads();
     if (tid < 8) {
-      double a = s_mx[tid * (PP_NT / 32)], b = s_mn[tid * (PP_NT / 32)];
-      for (int w = 1; w < PP_NT / 32; ++w) {
-        a = fmax(a, s_mx[tid * (PP_NT / 32) + w]);
-        b = fmin(b, s_mn[tid * (PP_NT / 32) + w]);
+      double sacc = 0.0;
+      for (int q = 0; q < ne; ++q) sacc = sacc + s_red[q * 8 + tid];
+      partial_out[tid] = sacc;
+      double a = s_red[TE * 8 + tid * 8], b = s_red[TE * 8 + 64 + tid * 8];
+      for (int w2 = 1; w2 < PP_NT / 32; ++w2) {
+        a = fmax(a, s_red[TE * 8 + tid * 8 + w2]);
+        b = fmin(b, s_red[TE * 8 + 64 + tid * 8 + w2]);
       }
       atomicMax(&ctrl->umax_bits[tid], ord_enc(a));
       atomicMin(&ctrl->umin_bits[tid], ord_enc(b));
     }
+    __syncthreads();  // s_red is reused by the next chunk
   }
 }
 
 template <int P>
+__device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s_A) {
+  constexpr int N2 = PPCfg<P>::N2;
+  for (int it = threadIdx.x; it < N2 * N2; it += PP_NT) s_A[it] = __ldg(A + it);
+}
+
+// one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once)
+template <int P>
 __global__ void __launch_bounds__(PP_NT)
     pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                       int gate, int apply_ldf, int need_global, int ent_offset,
-                      double* __restrict__ partial_sum,  // [gridDim.x][8]
+                      double* __restrict__ partial_sum,  // [chunks][8]
                       double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
-                      unsigned char* __restrict__ cell_ent_nan, int limit) {
+                      unsigned char* __restrict__ cell_ent_nan, int limit, int nchunks) {
+  using C = PPCfg<P>;
+  __shared__ double s_A[C::N2 * C::N2];
+  __shared__ double s_red[C::TE * 8 + 128];
+  __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
-  pp_avg_ldf_chunk<P>(u, u_avg, g, ctrl, blockIdx.x, apply_ldf, need_global, ent_offset,
-                      partial_sum + (long long)blockIdx.x * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit);
+  if (threadIdx.x == 0) s_cnt = 0;
+  if (apply_ldf) load_ldf<P>(g.ldfA, s_A);
+  __syncthreads();
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x)
+    pp_avg_ldf_chunk<P>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset, partial_sum + (long long)c * 8,
+                        cell_ent_DG, cell_ent_FV, cell_ent_nan, limit, s_A, s_red, &s_cnt);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
 }
 
 // many instances: items = every member's chunks; slot = the stage state; `final` selects the
@@ -377,15 +313,28 @@ template <int P>
 __global__ void __launch_bounds__(PP_NT)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+  using C = PPCfg<P>;
+  __shared__ double s_A[C::N2 * C::N2];
+  __shared__ double s_red[C::TE * 8 + 128];
+  __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
+  int loaded = -1;  // member whose LDF operator s_A holds
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
-    pp_avg_ldf_chunk<P>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, d.use_oedg && final,
-                        d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
-                        d.cell_ent_nan, !final);
+    if (threadIdx.x == 0) s_cnt = 0;
+    if (d.use_ldf && loaded != m) {
+      __syncthreads();
+      load_ldf<P>(d.g.ldfA, s_A);
+      loaded = m;
+    }
     __syncthreads();
+    pp_avg_ldf_chunk<P>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, d.use_oedg && final, d.ent_offset,
+                        d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan, !final, s_A,
+                        s_red, &s_cnt);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
 }
 
@@ -645,79 +594,82 @@ __device__ __forceinline__ void pp_limit_segment(
     int apply_oedg, double oedg_dt, int ent_offset, int comput_ent, const double* __restrict__ sig_x,
     const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
     const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
-    double* __restrict__ ent_out, double* __restrict__ accept_dst) {
+    double* __restrict__ ent_out, double* __restrict__ accept_dst, double* s_ent, int* s_cnt) {
   using C = PPCfg<P>;
-  constexpr int NN = C::NN, EB = C::EB, TE = C::TE;
+  constexpr int NN = C::NN, EB = C::EB, GS = C::GS, G = C::G, TE = C::TE;
   if (ctrl->neg_avg) return;  // the reference skips loop 3 once neg_avg is set (DG_solver.f90:431)
-  __shared__ __align__(16) double s_u[TE * EB];
-  __shared__ double s_avg[TE * 8];
-  __shared__ double s_nd[TE * NN * 2];  // per-node scratch (wave speeds, pressures, entropies)
-  __shared__ double s_theta[TE];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = lane / GS, node = lane - grp * GS;
   const int nx = g.nx, NXG = nx + 2;
   const int j = 1 + jrow;
   const int i0 = 1 + seg * TE;
   const int ne = min(TE, nx - i0 + 1);
-  const long long ebase = (long long)j * NXG + i0;
+  const int el = warp * G + grp;
+  const bool inside = el < ne, nd = node < NN;
+  const bool act = inside && nd;
+  const long long e = (long long)j * NXG + i0 + el;
   const double gamma = g.gamma;
-  for (int it = tid; it < ne * EB / 2; it += PP_NT)
-    reinterpret_cast<double2*>(s_u)[it] = reinterpret_cast<const double2*>(u + ebase * EB)[it];
-  for (int it = tid; it < ne * 8; it += PP_NT) s_avg[it] = u_avg[ebase * 8 + it];
-  __syncthreads();
-
+  double x[8], avg[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    x[v] = act ? u[e * EB + v * NN + node] : 0.0;
+    avg[v] = inside ? u_avg[e * 8 + v] : 1.0;
+  }
   if (apply_oedg) {  // DG_solver.f90:448-524
-    for (int it = tid; it < ne * NN; it += PP_NT) {
-      const int e = it / NN, q = it - e * NN;
-      const double* x = s_u + e * EB + q;
+    double sx = 0.0, sy = 0.0;
+    if (act) {
       const double rho = fmax(x[0], PP_EPS);
       const double ir = 1.0 / rho;
-      const double vx = ir * x[NN], vy = ir * x[2 * NN];
-      const double ek = 0.5 * ir * (x[NN] * x[NN] + x[2 * NN] * x[2 * NN] + x[3 * NN] * x[3 * NN]);
-      const double bx = x[4 * NN], by = x[5 * NN], bz = x[6 * NN];
+      const double vx = ir * x[1], vy = ir * x[2];
+      const double ek = 0.5 * ir * (x[1] * x[1] + x[2] * x[2] + x[3] * x[3]);
+      const double bx = x[4], by = x[5], bz = x[6];
       const double bsq = bx * bx + by * by + bz * bz;
-      const double pf = fmax((gamma - 1.0) * (x[7 * NN] - (ek + 0.5 * bsq)), PP_EPS);
+      const double pf = fmax((gamma - 1.0) * (x[7] - (ek + 0.5 * bsq)), PP_EPS);
       const double cs = gamma * pf * ir, ss = cs + bsq * ir, sqsq = ss * ss, coef = 4.0 * cs * ir;
-      s_nd[e * 2 * NN + q] = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(sqsq - coef * (bx * bx), 0.0)), 0.0));
-      s_nd[e * 2 * NN + NN + q] = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(sqsq - coef * (by * by), 0.0)), 0.0));
+      sx = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(sqsq - coef * (bx * bx), 0.0)), 0.0));
+      sy = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(sqsq - coef * (by * by), 0.0)), 0.0));
     }
-    __syncthreads();
-    if (tid < ne) {
-      const int e = tid, i = i0 + e;
-      double mx = 0.0, my = 0.0;
-      for (int q = 0; q < NN; ++q) {
-        mx = fmax(mx, s_nd[e * 2 * NN + q]);
-        my = fmax(my, s_nd[e * 2 * NN + NN + q]);
-      }
+    const double mx = grp_max<GS>(sx), my = grp_max<GS>(sy);
+    // lane `node` of the group forms delta_v for v = node, node + GS, ... from the element's four faces
+    double d = -1.0e308;
+    if (inside) {
+      const int i = i0 + el;
       const long long fxl = ((long long)(j - 1) * (nx + 1) + (i - 1)) * 8;
       const long long fyb = ((long long)(j - 1) * nx + (i - 1)) * 8;
       const long long fyt = ((long long)j * nx + (i - 1)) * 8;
-      double dmaxv = -1.0e308;
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
+      for (int v = node; v < 8; v += GS) {
         const double uv = ctrl->u_vari[v];
-        double d = 0.0;
+        double dv = 0.0;
         if (uv > OEDG_EPS)
-          d = ((mx / g.hx) * (sig_x[fxl + v] + sig_x[fxl + 8 + v]) + (my / g.hy) * (sig_y[fyb + v] + sig_y[fyt + v])) / uv;
-        dmaxv = fmax(dmaxv, d);
+          dv = ((mx / g.hx) * (sig_x[fxl + v] + sig_x[fxl + 8 + v]) + (my / g.hy) * (sig_y[fyb + v] + sig_y[fyt + v])) / uv;
+        d = fmax(d, dv);
       }
-      s_theta[e] = exp(-oedg_dt * dmaxv);
     }
-    __syncthreads();
-    for (int it = tid; it < ne * EB; it += PP_NT) {
-      const int e = it / EB, v = (it - e * EB) / NN;
-      const double a = s_avg[e * 8 + v];
-      s_u[it] = a + s_theta[e] * (s_u[it] - a);
-    }
-    __syncthreads();
+    const double dmax = grp_max<GS>(d);
+    const double theta = exp(-oedg_dt * dmax);
+    if (act)
+#pragma unroll
+      for (int v = 0; v < 8; ++v) x[v] = avg[v] + theta * (x[v] - avg[v]);
   }
-
-  limit_elements<P>(s_u, s_avg, nullptr, ne, ebase, g, ctrl, ent_offset, comput_ent, cell_ent_DG, cell_ent_FV,
-                    cell_ent_nan, ent_out);
-
-  for (int it = tid; it < ne * EB / 2; it += PP_NT) {
-    const double2 val = reinterpret_cast<const double2*>(s_u)[it];
-    reinterpret_cast<double2*>(u + ebase * EB)[it] = val;
-    if (accept_dst) reinterpret_cast<double2*>(accept_dst + ebase * EB)[it] = val;
+  bool neg = false;
+  const double ce = limit_group<P>(x, avg, act, inside && node == 0, node, e, g, ctrl, ent_offset, comput_ent,
+                                   cell_ent_DG, cell_ent_FV, cell_ent_nan, &neg);
+  const unsigned cnt = __popc(__ballot_sync(FULL_MASK, neg));
+  if (lane == 0 && cnt) atomicAdd(s_cnt, (int)cnt);
+  if (act)
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      u[e * EB + v * NN + node] = x[v];
+      if (accept_dst) accept_dst[e * EB + v * NN + node] = x[v];
+    }
+  if (comput_ent) {  // chunk partial in element order
+    if (inside && node == 0) s_ent[el] = ce;
+    __syncthreads();
+    if (tid == 0) {
+      double tot = 0.0;
+      for (int q = 0; q < ne; ++q) tot = tot + s_ent[q];
+      *ent_out = tot;
+    }
   }
 }
 
@@ -729,11 +681,17 @@ __global__ void __launch_bounds__(PP_NT)
                     const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
                     const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
                     double* __restrict__ ent_partial, double* __restrict__ accept_dst) {
+  __shared__ double s_ent[PPCfg<P>::TE];
+  __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
   const double oedg_dt = dt_ptr ? *dt_ptr : oedg_dt_arg;
   pp_limit_segment<P>(u, u_avg, g, ctrl, blockIdx.x, blockIdx.y, apply_oedg, oedg_dt, ent_offset, comput_ent,
                       sig_x, sig_y, cell_ent_DG, cell_ent_FV, cell_ent_nan,
-                      ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst);
+                      ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst, s_ent, &s_cnt);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
 }
 
 // many instances: items = every member's row segments (row-major); the final stage applies OEDG
@@ -742,17 +700,22 @@ template <int P>
 __global__ void __launch_bounds__(PP_NT)
     pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+  __shared__ double s_ent[PPCfg<P>::TE];
+  __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
     const int nseg = (d.g.nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE;
     const int seg = local % nseg, row = local / nseg;
     pp_limit_segment<P>(d.u[slot], d.u_avg, d.g, d.ctrl, seg, row, d.use_oedg && final, d.ctrl->dt,
                         d.ent_offset, final, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
-                        d.ent_partial + local, final ? d.u[0] : nullptr);
+                        d.ent_partial + local, final ? d.u[0] : nullptr, s_ent, &s_cnt);
     __syncthreads();
+    if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
 }
 
