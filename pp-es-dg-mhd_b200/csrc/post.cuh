@@ -26,6 +26,7 @@
 namespace mhd {
 
 constexpr int PP_NT = 256;
+constexpr int PP_MINB = 4;  // CTAs per SM the loop-1/loop-3 kernels are register-budgeted for
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 template <int P>
@@ -285,7 +286,7 @@ __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s
 
 // one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once)
 template <int P>
-__global__ void __launch_bounds__(PP_NT)
+__global__ void __launch_bounds__(PP_NT, PP_MINB)
     pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                       int gate, int apply_ldf, int need_global, int ent_offset,
                       double* __restrict__ partial_sum,  // [chunks][8]
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(PP_NT)
 // final-stage form (OEDG global reductions for instances that use OEDG); the other stages fuse
 // loop 3 (limit)
 template <int P>
-__global__ void __launch_bounds__(PP_NT)
+__global__ void __launch_bounds__(PP_NT, PP_MINB)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   using C = PPCfg<P>;
@@ -674,7 +675,7 @@ __device__ __forceinline__ void pp_limit_segment(
 }
 
 template <int P>
-__global__ void __launch_bounds__(PP_NT)
+__global__ void __launch_bounds__(PP_NT, PP_MINB)
     pp_limit_kernel(double* __restrict__ u, const double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                     int gate, int apply_oedg, const double* __restrict__ dt_ptr, double oedg_dt_arg,
                     int ent_offset, int comput_ent, const double* __restrict__ sig_x,
@@ -697,7 +698,7 @@ __global__ void __launch_bounds__(PP_NT)
 // many instances: items = every member's row segments (row-major); the final stage applies OEDG
 // (if the instance uses it), computes the entropy and writes the accepted interior into slot 0
 template <int P>
-__global__ void __launch_bounds__(PP_NT)
+__global__ void __launch_bounds__(PP_NT, PP_MINB)
     pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   __shared__ double s_ent[PPCfg<P>::TE];

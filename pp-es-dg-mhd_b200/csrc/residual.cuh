@@ -21,12 +21,23 @@ namespace mhd {
 // Tile (TX x TY elements), threads per CTA and the CTAs per SM the register budget is cut for.
 template <int P>
 struct ResCfg;
+// HW = warps that start phase 2 on the interface fluxes (the rest start on the node pairs, which
+// every warp then shares through a shared-memory work counter).
+#ifndef MHD_RES_HW1
+#define MHD_RES_HW1 3
+#endif
+#ifndef MHD_RES_HW2
+#define MHD_RES_HW2 2
+#endif
+#ifndef MHD_RES_HW3
+#define MHD_RES_HW3 3
+#endif
 template <>
-struct ResCfg<1> { static constexpr int TX = 8, TY = 4, NT = 128, MINB = 4; };
+struct ResCfg<1> { static constexpr int TX = 8, TY = 4, NT = 128, MINB = 4, HW = MHD_RES_HW1; };
 template <>
-struct ResCfg<2> { static constexpr int TX = 4, TY = 4, NT = 128, MINB = 4; };
+struct ResCfg<2> { static constexpr int TX = 4, TY = 4, NT = 128, MINB = 4, HW = MHD_RES_HW2; };
 template <>
-struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 128, MINB = 4; };
+struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 128, MINB = 4, HW = MHD_RES_HW3; };
 
 template <int P>
 struct ResLayout {
@@ -38,11 +49,8 @@ struct ResLayout {
   static constexpr int NFX = (TX + 1) * TY * N;
   static constexpr int NFY = TX * (TY + 1) * N;
   static constexpr int FW = 11;  // face record: flux[8], nB, sl, sr (stored component-major)
-  // threads of phase 2 given to the face nodes: a whole number of warps, cost-proportional
-  static constexpr int NT_ = ResCfg<P>::NT;
-  static constexpr int THL_RAW = (NT_ * (NFX + NFY) * 9) / ((NFX + NFY) * 9 + TE * NPAIR * 5);
-  static constexpr int THL_W = (THL_RAW + 16) / 32 * 32;
-  static constexpr int THL = THL_W < 32 ? 32 : (THL_W > NT_ - 32 ? NT_ - 32 : THL_W);
+  static constexpr int THL = 32 * ResCfg<P>::HW;  // threads that start phase 2 on the face nodes
+  static_assert(ResCfg<P>::HW >= 1 && THL <= ResCfg<P>::NT, "face warps must fit the CTA");
   // offsets in doubles
   static constexpr int O_CONS = 0;
   static constexpr int O_PRIM = O_CONS + TE * EB;
@@ -55,7 +63,7 @@ struct ResLayout {
   static constexpr int O_PAIR = O_FY + NFY * FW;
   static constexpr int O_SIG = O_PAIR + TE * NPAIR * 8;
   static constexpr int O_RED = O_SIG + TE * 2 * NN;
-  static constexpr int TOTAL = O_RED + 32;
+  static constexpr int TOTAL = O_RED + 32;  // O_RED + 16 doubles also hold the pair work counter
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
 };
 
@@ -90,6 +98,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   double* s_pair = sm + L::O_PAIR;
   double* s_sig = sm + L::O_SIG;
   double* s_red = sm + L::O_RED;
+  int* s_next = reinterpret_cast<int*>(s_red + 16);  // next node-pair chunk of phase 2
 
   const int tid = threadIdx.x;
   const int nx = g.nx, ny = g.ny;
@@ -99,6 +108,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   const double gamma = g.gamma;
 
   // ---- phase 0: load the tile and its halo traces ----
+  if (tid == 0) *s_next = 0;
   {
     constexpr int V2 = TX * EB / 2;  // double2 per tile row
     for (int it = tid; it < H * V2; it += NT) {
@@ -156,19 +166,16 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   __syncthreads();
 
   // ---- phase 2: interface fluxes and element pair fluxes ----
-  // Warp-specialised: the first THL threads (whole warps) take the face nodes, the others the
-  // node pairs, split in proportion to their cost (one HLL flux ~ 1.8 EC fluxes).
+  // The first THL threads (whole warps) take the face nodes; all warps take the node pairs in
+  // chunks of 32 from a shared counter (the face warps once their faces are done), so the two
+  // kinds of work balance whatever their relative cost.
   {
     constexpr int NH = L::NFX + L::NFY, NPT = TE * L::NPAIR;
     constexpr int THL = L::THL;
-    const bool hll_thread = tid < THL;
-    const int first = hll_thread ? tid : NH + (tid - THL);
-    const int stride = hll_thread ? THL : NT - THL;
-    const int last = hll_thread ? NH : NH + NPT;
-    for (int it = first; it < last; it += stride) {
+    auto face_node = [&](int it) {
       if (it < L::NFX) {  // x face node
         const int fi = it / (TY * N), rem = it - fi * TY * N, r = rem / N, l = rem - r * N;
-        if (r >= H || fi > W) continue;
+        if (r >= H || fi > W) return;
         double wl[8], wr[8];
 #pragma unroll
         for (int v = 0; v < 8; ++v) {
@@ -182,7 +189,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       } else if (it < L::NFX + L::NFY) {  // y face node (swap_xy in and out)
         const int f = it - L::NFX;
         const int fj = f / (TX * N), rem = f - fj * TX * N, c = rem / N, k = rem - c * N;
-        if (c >= W || fj > H) continue;
+        if (c >= W || fj > H) return;
         double a[8], b[8];
 #pragma unroll
         for (int v = 0; v < 8; ++v) {
@@ -205,11 +212,12 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
         dst[8 * L::NFY] = o[8];
         dst[9 * L::NFY] = o[9];
         dst[10 * L::NFY] = o[10];
-      } else {  // element node pair
-        const int pidx = it - L::NFX - L::NFY;
+      }
+    };
+    auto node_pair = [&](int pidx) {  // element node pair
         const int e = pidx / L::NPAIR, pi = pidx - e * L::NPAIR;
         const int er = e / TX, ec = e - er * TX;
-        if (er >= H || ec >= W) continue;
+        if (er >= H || ec >= W) return;
         const double* pb = s_prim + e * EB;
         double A[8], B[8], F[8];
         if (pi < L::NPX) {  // x pair on line l: nodes (a,l) [the reference's k] and (b,l) [r]
@@ -237,7 +245,15 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
         double* dst = s_pair + e * L::NPAIR + pi;  // variable-major: no bank conflicts
 #pragma unroll
         for (int v = 0; v < 8; ++v) dst[v * TE * L::NPAIR] = F[v];
-      }
+    };
+    if (tid < THL)
+      for (int it = tid; it < NH; it += THL) face_node(it);
+    for (;;) {
+      int base = 0;
+      if ((tid & 31) == 0) base = atomicAdd(s_next, 32);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= NPT) break;
+      if (base + (tid & 31) < NPT) node_pair(base + (tid & 31));
     }
   }
   __syncthreads();
