@@ -78,6 +78,9 @@ __device__ __forceinline__ void pair_ab(int idx, int& a, int& b) {
 }
 __device__ __forceinline__ int pair_index(int a, int b) { return a * (a - 1) / 2 + b; }
 
+// swap_xy (DG_solver.f90:1556-1568) as a variable permutation: 1 <-> 2, 4 <-> 5
+__host__ __device__ constexpr int swap_xy_var(int v) { return v == 1 ? 2 : v == 2 ? 1 : v == 4 ? 5 : v == 5 ? 4 : v; }
+
 // One tile of the residual: elements (tile_x*TX + 1 .. , tile_y*TY + 1 .. ) of the instance
 // described by (u, ut, g, ctrl).  All threads of the CTA call it with the same arguments.
 template <int P>
@@ -172,79 +175,72 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   {
     constexpr int NH = L::NFX + L::NFY, NPT = TE * L::NPAIR;
     constexpr int THL = L::THL;
+    // One call site per flux: a y face or y pair is rotated into the x frame by swap_xy (the
+    // component permutation 1<->2, 4<->5, its own inverse) on the way in and out, as the
+    // reference does for faces (DG_solver.f90:1556-1568); both fluxes are exactly covariant
+    // under it, so the result equals the y-direction formula bit for bit.
     auto face_node = [&](int it) {
-      if (it < L::NFX) {  // x face node
+      const bool ydir = it >= L::NFX;
+      const double *pl, *pr;
+      int sl, sr;  // variable strides of the two traces
+      double* dst;
+      int ostride;
+      if (!ydir) {  // x face node: left/right traces of row r, face fi, node l
         const int fi = it / (TY * N), rem = it - fi * TY * N, r = rem / N, l = rem - r * N;
         if (r >= H || fi > W) return;
-        double wl[8], wr[8];
-#pragma unroll
-        for (int v = 0; v < 8; ++v) {
-          wl[v] = (fi == 0) ? s_hxl[(r * 8 + v) * N + l] : s_cons[(r * TX + fi - 1) * EB + v * NN + (N - 1) + N * l];
-          wr[v] = (fi == W) ? s_hxr[(r * 8 + v) * N + l] : s_cons[(r * TX + fi) * EB + v * NN + N * l];
-        }
-        double o[11];
-        espp_hll(wl, wr, gamma, o);
-#pragma unroll
-        for (int c = 0; c < L::FW; ++c) s_fx[c * L::NFX + it] = o[c];  // component-major: no bank conflicts
-      } else if (it < L::NFX + L::NFY) {  // y face node (swap_xy in and out)
+        if (fi == 0) { pl = s_hxl + r * 8 * N + l; sl = N; }
+        else { pl = s_cons + (r * TX + fi - 1) * EB + (N - 1) + N * l; sl = NN; }
+        if (fi == W) { pr = s_hxr + r * 8 * N + l; sr = N; }
+        else { pr = s_cons + (r * TX + fi) * EB + N * l; sr = NN; }
+        dst = s_fx + it;
+        ostride = L::NFX;
+      } else {  // y face node: bottom/top traces of column c, face fj, node k
         const int f = it - L::NFX;
         const int fj = f / (TX * N), rem = f - fj * TX * N, c = rem / N, k = rem - c * N;
         if (c >= W || fj > H) return;
-        double a[8], b[8];
-#pragma unroll
-        for (int v = 0; v < 8; ++v) {
-          a[v] = (fj == 0) ? s_hyb[(c * 8 + v) * N + k] : s_cons[((fj - 1) * TX + c) * EB + v * NN + k + N * (N - 1)];
-          b[v] = (fj == H) ? s_hyt[(c * 8 + v) * N + k] : s_cons[(fj * TX + c) * EB + v * NN + k];
-        }
-        double sa[8] = {a[0], a[2], a[1], a[3], a[5], a[4], a[6], a[7]};
-        double sb[8] = {b[0], b[2], b[1], b[3], b[5], b[4], b[6], b[7]};
-        double o[11];
-        espp_hll(sa, sb, gamma, o);
-        double* dst = s_fy + f;
-        dst[0 * L::NFY] = o[0];
-        dst[1 * L::NFY] = o[2];
-        dst[2 * L::NFY] = o[1];
-        dst[3 * L::NFY] = o[3];
-        dst[4 * L::NFY] = o[5];
-        dst[5 * L::NFY] = o[4];
-        dst[6 * L::NFY] = o[6];
-        dst[7 * L::NFY] = o[7];
-        dst[8 * L::NFY] = o[8];
-        dst[9 * L::NFY] = o[9];
-        dst[10 * L::NFY] = o[10];
+        if (fj == 0) { pl = s_hyb + c * 8 * N + k; sl = N; }
+        else { pl = s_cons + ((fj - 1) * TX + c) * EB + k + N * (N - 1); sl = NN; }
+        if (fj == H) { pr = s_hyt + c * 8 * N + k; sr = N; }
+        else { pr = s_cons + (fj * TX + c) * EB + k; sr = NN; }
+        dst = s_fy + f;
+        ostride = L::NFY;
       }
+      double wl[8], wr[8], o[11];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        const int sv = ydir ? swap_xy_var(v) : v;
+        wl[v] = pl[sv * sl];
+        wr[v] = pr[sv * sr];
+      }
+      espp_hll(wl, wr, gamma, o);
+#pragma unroll
+      for (int c = 0; c < L::FW; ++c) dst[(ydir && c < 8 ? swap_xy_var(c) : c) * ostride] = o[c];  // component-major
     };
     auto node_pair = [&](int pidx) {  // element node pair
-        const int e = pidx / L::NPAIR, pi = pidx - e * L::NPAIR;
-        const int er = e / TX, ec = e - er * TX;
-        if (er >= H || ec >= W) return;
-        const double* pb = s_prim + e * EB;
-        double A[8], B[8], F[8];
-        if (pi < L::NPX) {  // x pair on line l: nodes (a,l) [the reference's k] and (b,l) [r]
-          const int l = pi / L::NPR;
-          int a, b;
-          pair_ab(pi - l * L::NPR, a, b);
+      const int e = pidx / L::NPAIR, pi = pidx - e * L::NPAIR;
+      const int er = e / TX, ec = e - er * TX;
+      if (er >= H || ec >= W) return;
+      const bool ydir = pi >= L::NPX;
+      const int pj = ydir ? pi - L::NPX : pi;
+      const int line = pj / L::NPR;
+      int a, b;
+      pair_ab(pj - line * L::NPR, a, b);
+      // x pair on line l: nodes (a,l) [the reference's k] and (b,l) [r];
+      // y pair on column k: nodes (k,a) [the reference's l] and (k,b) [s]
+      const double* pb = s_prim + e * EB;
+      const double* pA = pb + (ydir ? line + N * a : a + N * line);
+      const double* pB = pb + (ydir ? line + N * b : b + N * line);
+      double A[8], B[8], F[8];
 #pragma unroll
-          for (int v = 0; v < 8; ++v) {
-            A[v] = pb[v * NN + a + N * l];
-            B[v] = pb[v * NN + b + N * l];
-          }
-          ec_flux<0>(A, B, gamma, F);
-        } else {  // y pair on column k: nodes (k,a) [the reference's l] and (k,b) [s]
-          const int pj = pi - L::NPX;
-          const int k = pj / L::NPR;
-          int a, b;
-          pair_ab(pj - k * L::NPR, a, b);
+      for (int v = 0; v < 8; ++v) {
+        const int sv = ydir ? swap_xy_var(v) : v;
+        A[v] = pA[sv * NN];
+        B[v] = pB[sv * NN];
+      }
+      ec_flux<0>(A, B, gamma, F);
+      double* dst = s_pair + e * L::NPAIR + pi;  // variable-major: no bank conflicts
 #pragma unroll
-          for (int v = 0; v < 8; ++v) {
-            A[v] = pb[v * NN + k + N * a];
-            B[v] = pb[v * NN + k + N * b];
-          }
-          ec_flux<1>(A, B, gamma, F);
-        }
-        double* dst = s_pair + e * L::NPAIR + pi;  // variable-major: no bank conflicts
-#pragma unroll
-        for (int v = 0; v < 8; ++v) dst[v * TE * L::NPAIR] = F[v];
+      for (int v = 0; v < 8; ++v) dst[(ydir ? swap_xy_var(v) : v) * TE * L::NPAIR] = F[v];
     };
     if (tid < THL)
       for (int it = tid; it < NH; it += THL) face_node(it);
