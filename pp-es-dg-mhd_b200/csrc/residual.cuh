@@ -335,28 +335,19 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
       }
-      // surface terms (DG_solver.f90:872-882)
-      if (k == 0) {
-        const double* fr = s_fx + ((ec * TY + er) * N + l);
-        const double c = sxh / dc.qw[0];
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
-      }
-      if (k == N - 1) {
-        const double* fr = s_fx + (((ec + 1) * TY + er) * N + l);
-        const double c = sxh / dc.qw[N - 1];
+      // surface terms (DG_solver.f90:872-882): the left face (k = 0) enters with -, the right
+      // face (k = N-1) with +; likewise bottom/top in y.  One block per direction.
+      if (k == 0 || k == N - 1) {
+        const bool right = (k == N - 1) && (N > 1);
+        const double* fr = s_fx + (((ec + (right ? 1 : 0)) * TY + er) * N + l);
+        const double c = (right ? sxh : -sxh) / dc.qw[k];
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
       }
-      if (l == 0) {
-        const double* fr = s_fy + ((er * TX + ec) * N + k);
-        const double c = syh / dc.qw[0];
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
-      }
-      if (l == N - 1) {
-        const double* fr = s_fy + (((er + 1) * TX + ec) * N + k);
-        const double c = syh / dc.qw[N - 1];
+      if (l == 0 || l == N - 1) {
+        const bool top = (l == N - 1) && (N > 1);
+        const double* fr = s_fy + (((er + (top ? 1 : 0)) * TX + ec) * N + k);
+        const double c = (top ? syh : -syh) / dc.qw[l];
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
       }
