@@ -42,6 +42,10 @@ struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 128, MINB = 4, HW =
 template <int P>
 struct ResLayout {
   static constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
+  // shared element records padded by 16 bytes for p = 1 and 3, so that the same node of
+  // neighbouring elements falls in different banks (face traces are read across elements); at
+  // p = 2 the unpadded 576-byte record measured faster
+  static constexpr int ES = EB + (P == 2 ? 0 : 2);
   static constexpr int TX = ResCfg<P>::TX, TY = ResCfg<P>::TY, TE = TX * TY;
   static constexpr int NPR = N * (N - 1) / 2;  // pairs per line
   static constexpr int NPX = N * NPR;          // x pairs per element
@@ -53,8 +57,8 @@ struct ResLayout {
   static_assert(ResCfg<P>::HW >= 1 && THL <= ResCfg<P>::NT, "face warps must fit the CTA");
   // offsets in doubles
   static constexpr int O_CONS = 0;
-  static constexpr int O_PRIM = O_CONS + TE * EB;
-  static constexpr int O_HXL = O_PRIM + TE * EB;
+  static constexpr int O_PRIM = O_CONS + TE * ES;
+  static constexpr int O_HXL = O_PRIM + TE * ES;
   static constexpr int O_HXR = O_HXL + TY * 8 * N;
   static constexpr int O_HYB = O_HXR + TY * 8 * N;
   static constexpr int O_HYT = O_HYB + TX * 8 * N;
@@ -88,7 +92,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
                                               const Geo& g, Ctrl* ctrl, int tile_x, int tile_y,
                                               double* sm) {
   using L = ResLayout<P>;
-  constexpr int N = L::N, NN = L::NN, EB = L::EB, TX = L::TX, TY = L::TY, TE = L::TE;
+  constexpr int N = L::N, NN = L::NN, EB = L::EB, ES = L::ES, TX = L::TX, TY = L::TY, TE = L::TE;
   constexpr int NT = ResCfg<P>::NT;
   double* s_cons = sm + L::O_CONS;
   double* s_prim = sm + L::O_PRIM;
@@ -118,7 +122,8 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       const int r = it / V2, c = it - r * V2;
       if (c < W * EB / 2) {
         const double2* src = reinterpret_cast<const double2*>(u + (long long)(j0 + r) * rowstride + (long long)i0 * EB);
-        reinterpret_cast<double2*>(s_cons + r * TX * EB)[c] = __ldg(src + c);
+        const int ec = (ES == EB) ? 0 : c / (EB / 2), cw = c - ec * (EB / 2);  // unpadded: one run
+        reinterpret_cast<double2*>(s_cons + (r * TX + ec) * ES)[cw] = __ldg(src + c);
       }
     }
     for (int it = tid; it < TY * 8 * N; it += NT) {  // x halos: traces k = n-1 (left) / 0 (right)
@@ -144,7 +149,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
     const int e = it / NN, q = it - e * NN;
     const int er = e / TX, ec = e - er * TX;
     if (er >= H || ec >= W) continue;
-    const double* w0 = s_cons + e * EB + q;
+    const double* w0 = s_cons + e * ES + q;
     double w[8];
 #pragma unroll
     for (int v = 0; v < 8; ++v) w[v] = w0[v * NN];
@@ -153,7 +158,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
     const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
     const double bsq = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
     const double pf = fmax((gamma - 1.0) * (w[7] - (ek + 0.5 * bsq)), PP_EPS);
-    double* pr = s_prim + e * EB + q;
+    double* pr = s_prim + e * ES + q;
     pr[0 * NN] = w[0];
     pr[1 * NN] = vx;
     pr[2 * NN] = vy;
@@ -189,9 +194,9 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
         const int fi = it / (TY * N), rem = it - fi * TY * N, r = rem / N, l = rem - r * N;
         if (r >= H || fi > W) return;
         if (fi == 0) { pl = s_hxl + r * 8 * N + l; sl = N; }
-        else { pl = s_cons + (r * TX + fi - 1) * EB + (N - 1) + N * l; sl = NN; }
+        else { pl = s_cons + (r * TX + fi - 1) * ES + (N - 1) + N * l; sl = NN; }
         if (fi == W) { pr = s_hxr + r * 8 * N + l; sr = N; }
-        else { pr = s_cons + (r * TX + fi) * EB + N * l; sr = NN; }
+        else { pr = s_cons + (r * TX + fi) * ES + N * l; sr = NN; }
         dst = s_fx + it;
         ostride = L::NFX;
       } else {  // y face node: bottom/top traces of column c, face fj, node k
@@ -199,9 +204,9 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
         const int fj = f / (TX * N), rem = f - fj * TX * N, c = rem / N, k = rem - c * N;
         if (c >= W || fj > H) return;
         if (fj == 0) { pl = s_hyb + c * 8 * N + k; sl = N; }
-        else { pl = s_cons + ((fj - 1) * TX + c) * EB + k + N * (N - 1); sl = NN; }
+        else { pl = s_cons + ((fj - 1) * TX + c) * ES + k + N * (N - 1); sl = NN; }
         if (fj == H) { pr = s_hyt + c * 8 * N + k; sr = N; }
-        else { pr = s_cons + (fj * TX + c) * EB + k; sr = NN; }
+        else { pr = s_cons + (fj * TX + c) * ES + k; sr = NN; }
         dst = s_fy + f;
         ostride = L::NFY;
       }
@@ -227,7 +232,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       pair_ab(pj - line * L::NPR, a, b);
       // x pair on line l: nodes (a,l) [the reference's k] and (b,l) [r];
       // y pair on column k: nodes (k,a) [the reference's l] and (k,b) [s]
-      const double* pb = s_prim + e * EB;
+      const double* pb = s_prim + e * ES;
       const double* pA = pb + (ydir ? line + N * a : a + N * line);
       const double* pB = pb + (ydir ? line + N * b : b + N * line);
       double A[8], B[8], F[8];
@@ -264,8 +269,8 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       const int er = e / TX, ec = e - er * TX;
       if (er >= H || ec >= W) continue;
       const int k = q % N, l = q / N;
-      double* cw = s_cons + e * EB + q;
-      const double* pb = s_prim + e * EB;
+      double* cw = s_cons + e * ES + q;
+      const double* pb = s_prim + e * ES;
       double w[8];
 #pragma unroll
       for (int v = 0; v < 8; ++v) w[v] = cw[v * NN];
@@ -394,7 +399,8 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       const int r = it / V2, c = it - r * V2;
       if (c < W * EB / 2) {
         double2* dst = reinterpret_cast<double2*>(ut + ((long long)(j0 + r - 1) * nx + (i0 - 1)) * EB);
-        dst[c] = reinterpret_cast<const double2*>(s_cons + r * TX * EB)[c];
+        const int ec = (ES == EB) ? 0 : c / (EB / 2), cw = c - ec * (EB / 2);
+        dst[c] = reinterpret_cast<const double2*>(s_cons + (r * TX + ec) * ES)[cw];
       }
     }
   }
