@@ -393,116 +393,73 @@ __global__ void __launch_bounds__(256) pp_reduce_batched(const InstDesc* __restr
 // shared memory with coalesced loads; each (face, variable) item then reads two variable blocks.
 // Shared records are padded (NN+1 doubles per variable) against bank conflicts.
 // ---------------------------------------------------------------------------------------------
-// x face: L, R = the variable's nodes [k + N*l] of the left and right element
+// One face, either direction.  Rp, Lm = the variable's nodes of the element after and before the
+// face (its first trace, R0, and last trace, RN, along the normal); node (a along the normal, b
+// along the face) sits at a*sn + b*st (x face: sn = 1, st = N; y face: sn = N, st = 1).  sn_h,
+// st_h = 2/h along the normal and along the face; coef[n][t] = (2(n+t)+1) h^(n+t) / (2 max(2p-1,1)
+// n! t!) with h the element size along the normal.  The x face of the reference (DG_solver.f90:
+// 296-343) is this with (R, L, hx, hy); its y face (:360-407) with (T, B, hy, hx): the two loops
+// are the same arithmetic with the roles of the directions exchanged.
 template <int P>
-__device__ __forceinline__ double sigsum_x_face(const double* R, const double* Lf, double hx, double hy) {
+__device__ __forceinline__ double sigsum_face(const double* Rp, const double* Lm, int sn, int st, double sn_h,
+                                              double st_h, const double* coef) {
   constexpr int N = P + 1;
   const DegConst& dc = c_deg[P];
-  const int denom_base = 2 * max(2 * P - 1, 1);
-  const double sx = 2.0 / hx, sy = 2.0 / hy;
   double total = 0.0;
-  double sxk = 1.0, hx_pow_kk = 1.0;
-  int fac_kk = 1;
+  double snk = 1.0;
 #pragma unroll 1
   for (int kk = 0; kk <= P; ++kk) {
     double jump[N];
 #pragma unroll
-    for (int l = 0; l < N; ++l) {
+    for (int b = 0; b < N; ++b) {
       double tr = 0.0, tl = 0.0;
 #pragma unroll
-      for (int k = 0; k < N; ++k) {
-        tr += dc.R0[kk][k] * R[k + N * l];
-        tl += dc.RN[kk][k] * Lf[k + N * l];
+      for (int a = 0; a < N; ++a) {
+        tr += dc.R0[kk][a] * Rp[a * sn + b * st];
+        tl += dc.RN[kk][a] * Lm[a * sn + b * st];
       }
-      jump[l] = sxk * tr - sxk * tl;
+      jump[b] = snk * tr - snk * tl;
     }
-    int fac_ll = 1;
-    double h_pow = hx_pow_kk;
 #pragma unroll
-    for (int ll = 0; ll <= P - kk; ++ll) {
+    for (int ll = 0; ll <= P; ++ll) {
+      if (ll > P - kk) break;
       double L1 = 0.0;
 #pragma unroll
-      for (int l = 0; l < N; ++l) L1 += (0.5 * dc.qw[l]) * fabs(jump[l]);
-      const double coef = ((2 * (kk + ll) + 1) * h_pow) / (double)(denom_base * fac_kk * fac_ll);
-      total = total + coef * L1;
-      if (ll < P) {
+      for (int b = 0; b < N; ++b) L1 += (0.5 * dc.qw[b]) * fabs(jump[b]);
+      total = total + coef[kk * N + ll] * L1;
+      if (ll < P - kk) {  // tangential derivative for the next order
         double nj[N];
 #pragma unroll
         for (int a = 0; a < N; ++a) {
           double acc = 0.0;
 #pragma unroll
-          for (int b = 0; b < N; ++b) acc += (sy * dc.D[a + N * b]) * jump[b];
+          for (int b = 0; b < N; ++b) acc += (st_h * dc.D[a + N * b]) * jump[b];
           nj[a] = acc;
         }
 #pragma unroll
         for (int a = 0; a < N; ++a) jump[a] = nj[a];
-        fac_ll *= (ll + 1);
-        h_pow *= hx;
       }
     }
-    if (kk < P) {
-      fac_kk *= (kk + 1);
-      hx_pow_kk *= hx;
-      sxk *= sx;
-    }
+    snk *= sn_h;
   }
   return total;
 }
 
-// y face: B, T = the variable's nodes of the bottom and top element
+// coef[n][t] of sigsum_face for element size h (the reference's running products h^(n+t), n! t!)
 template <int P>
-__device__ __forceinline__ double sigsum_y_face(const double* T, const double* B, double hx, double hy) {
-  constexpr int N = P + 1;
-  const DegConst& dc = c_deg[P];
+__device__ __forceinline__ double sigsum_coef(int n, int t, double h) {
   const int denom_base = 2 * max(2 * P - 1, 1);
-  const double sx = 2.0 / hx, sy = 2.0 / hy;
-  double total = 0.0;
-  double syl = 1.0, hy_pow_ll = 1.0;
-  int fac_ll = 1;
-#pragma unroll 1
-  for (int ll = 0; ll <= P; ++ll) {
-    double jump[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-      double tt = 0.0, tb = 0.0;
-#pragma unroll
-      for (int l = 0; l < N; ++l) {
-        tt += dc.R0[ll][l] * T[k + N * l];
-        tb += dc.RN[ll][l] * B[k + N * l];
-      }
-      jump[k] = syl * tt - syl * tb;
-    }
-    int fac_kk = 1;
-    double h_pow = hy_pow_ll;
-#pragma unroll
-    for (int kk = 0; kk <= P - ll; ++kk) {
-      double L1 = 0.0;
-#pragma unroll
-      for (int k = 0; k < N; ++k) L1 += (0.5 * dc.qw[k]) * fabs(jump[k]);
-      const double coef = ((2 * (kk + ll) + 1) * h_pow) / (double)(denom_base * fac_kk * fac_ll);
-      total = total + coef * L1;
-      if (kk < P) {
-        double nj[N];
-#pragma unroll
-        for (int a = 0; a < N; ++a) {
-          double acc = 0.0;
-#pragma unroll
-          for (int b = 0; b < N; ++b) acc += (sx * dc.D[a + N * b]) * jump[b];
-          nj[a] = acc;
-        }
-#pragma unroll
-        for (int a = 0; a < N; ++a) jump[a] = nj[a];
-        fac_kk *= (kk + 1);
-        h_pow *= hy;
-      }
-    }
-    if (ll < P) {
-      fac_ll *= (ll + 1);
-      hy_pow_ll *= hy;
-      syl *= sy;
-    }
+  double hp = 1.0;
+  int fn = 1, ft = 1;
+  for (int i = 0; i < n; ++i) {
+    hp *= h;
+    fn *= (i + 1);
   }
-  return total;
+  for (int i = 0; i < t; ++i) {
+    hp *= h;
+    ft *= (i + 1);
+  }
+  return ((2 * (n + t) + 1) * hp) / (double)(denom_base * fn * ft);
 }
 
 template <int P>
@@ -543,6 +500,13 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
     s_e[(rr * RW + cc) * ES + v * VS + q] = __ldg(u + ((long long)(j0 - 1 + rr) * NXG + (i0 - 1)) * EB + rem);
   }
   __syncthreads();
+  __shared__ double s_coef[2 * (P + 1) * (P + 1)];  // x faces (h = hx), then y faces (h = hy)
+  if (tid < 2 * (P + 1) * (P + 1)) {
+    const int d = tid / ((P + 1) * (P + 1)), r = tid - d * (P + 1) * (P + 1), n = r / (P + 1), t = r - n * (P + 1);
+    s_coef[tid] = (n + t <= P) ? sigsum_coef<P>(n, t, d == 0 ? g.hx : g.hy) : 0.0;
+  }
+  __syncthreads();
+  const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
   const int nfx = H * (W + right), nfy = W * (H + top);
   for (int it = tid; it < 8 * (nfx + nfy); it += NT) {
     const int v = it & 7, f = it >> 3;
@@ -550,13 +514,15 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
       const int r = f / (W + right), c = f - r * (W + right);
       const double* pl = s_e + ((r + 1) * RW + c) * ES + v * VS;
       const int i = i0 + c, j = j0 + r;
-      sig_x[(((long long)(j - 1) * (nx + 1)) + (i - 1)) * 8 + v] = sigsum_x_face<P>(pl + ES, pl, g.hx, g.hy);
+      sig_x[(((long long)(j - 1) * (nx + 1)) + (i - 1)) * 8 + v] =
+          sigsum_face<P>(pl + ES, pl, 1, P + 1, sxh, syh, s_coef);
     } else {  // y face: column c, face r between rows r-1 and r of the tile
       const int f2 = f - nfx;
       const int c = f2 / (H + top), r = f2 - c * (H + top);
       const double* pb = s_e + (r * RW + c + 1) * ES + v * VS;
       const int i = i0 + c, j = j0 + r;
-      sig_y[(((long long)(j - 1) * nx) + (i - 1)) * 8 + v] = sigsum_y_face<P>(pb + RW * ES, pb, g.hx, g.hy);
+      sig_y[(((long long)(j - 1) * nx) + (i - 1)) * 8 + v] =
+          sigsum_face<P>(pb + RW * ES, pb, P + 1, 1, syh, sxh, s_coef + (P + 1) * (P + 1));
     }
   }
 }
