@@ -188,7 +188,7 @@ int full_grid(K kernel, int threads, size_t smem, int nsm) {
 }
 
 struct BatchGrids {
-  int res, cmb, bc, avg, sig, lim;
+  int res, cmb, bc, avg, avg_final, sig, lim;
 };
 
 // queried before a capture begins (the occupancy calculator is host-only work)
@@ -199,7 +199,8 @@ BatchGrids batch_grids(int nsm) {
   gr.res = full_grid(residual_batched<P>, ResCfg<P>::NT, ResLayout<P>::BYTES, nsm);
   gr.cmb = full_grid(combine_batched<EB>, 256, 0, nsm);
   gr.bc = full_grid(bc_batched<P>, 256, 0, nsm);
-  gr.avg = full_grid(pp_avg_ldf_batched<P>, PP_NT, 0, nsm);
+  gr.avg = full_grid(pp_avg_ldf_batched<P, false>, PP_NT, 0, nsm);
+  gr.avg_final = full_grid(pp_avg_ldf_batched<P, true>, PP_NT, 0, nsm);
   gr.sig = full_grid(pp_sigsum_batched<P>, 256, 0, nsm);
   gr.lim = full_grid(pp_limit_batched<P>, PP_NT, 0, nsm);
   return gr;
@@ -223,7 +224,10 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_TIME, R, s);
     combine_batched<EB><<<grid_cmb, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
     bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
-    pp_avg_ldf_batched<P><<<grid_avg, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, fin, ST_RUN);
+    if (fin)
+      pp_avg_ldf_batched<P, true><<<gr.avg_final, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN);
+    else
+      pp_avg_ldf_batched<P, false><<<grid_avg, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN);
     if (fin) {
       pp_reduce_batched<<<b->nsm, 256, 0, st>>>(in, ninst, fin, ST_RUN);
       pp_sigsum_batched<P><<<grid_sig, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);

@@ -114,14 +114,14 @@ template <int P>
 dim3 pp_grid_limit(const mhd_gpu* h) { return dim3((h->nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE, h->ny); }
 
 // CTAs of pp_avg_ldf_kernel<P> the device holds at once (its grid walks the chunks)
-template <int P>
+template <int P, bool NEEDG>
 int pp_resident_ctas(int dev) {
   static int cached[kMaxDevices];
   if (dev < 0 || dev >= kMaxDevices) return 1;
   if (!cached[dev]) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pp_avg_ldf_kernel<P>, PP_NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pp_avg_ldf_kernel<P, NEEDG>, PP_NT, 0);
     cached[dev] = std::max(1, nsm) * std::max(1, per_sm);
   }
   return cached[dev];
@@ -222,10 +222,17 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
                  int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0) {
   const int nb1 = pp_nblk_avg<P>(h);
   const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
-  const int grid1 = std::min(nb1, pp_resident_ctas<P>(h->device));
-  pp_avg_ldf_kernel<P><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
-                                                        apply_oedg, ent_offset, h->partial, h->cell_ent_DG,
-                                                        h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
+  if (apply_oedg) {
+    const int grid1 = std::min(nb1, pp_resident_ctas<P, true>(h->device));
+    pp_avg_ldf_kernel<P, true><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
+                                                                1, ent_offset, h->partial, h->cell_ent_DG,
+                                                                h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
+  } else {
+    const int grid1 = std::min(nb1, pp_resident_ctas<P, false>(h->device));
+    pp_avg_ldf_kernel<P, false><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
+                                                                 0, ent_offset, h->partial, h->cell_ent_DG,
+                                                                 h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
+  }
   if (limit_in_loop1) return;
   if (apply_oedg) {
     pp_reduce_kernel<<<1, 256, 0, h->stream>>>(h->partial, nb1, h->ctrl, gate);

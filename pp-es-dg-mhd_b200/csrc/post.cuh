@@ -144,13 +144,14 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
 // on neg_avg (the time-step pipeline re-tries the step from u_con), so the stand-alone
 // post_process never fuses.
 // ---------------------------------------------------------------------------------------------
-template <int P>
+template <int P, bool NEEDG>
 __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg, const Geo& g,
                                                  Ctrl* ctrl, long long chunk, int apply_ldf, int need_global,
                                                  int ent_offset, double* __restrict__ partial_out,  // 8 doubles
                                                  double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                                                  unsigned char* __restrict__ cell_ent_nan, int limit,
-                                                 const double* s_A, double* s_red, int* s_cnt) {
+                                                 const double* s_A, double* s_red, int* s_cnt, double* run_max,
+                                                 double* run_min) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -222,27 +223,19 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
       x[5] = oy + avg[5];
     }
   }
-  if (need_global) {
+  if (NEEDG && need_global) {
     // chunk sum of (hx*hy)*avg over interior elements in element order (DG_solver.f90:227-229)
     if (el < TE)
 #pragma unroll
       for (int v = 0; v < 8; ++v)
         if (v % GS == node) s_red[el * 8 + v] = inner ? (g.hx * g.hy) * avg[v] : 0.0;
-    // max and min of the post-LDF interior node values
-    const bool use = inner && nd;
+    // running max and min of the post-LDF interior node values (reduced by flush_minmax)
+    if (inner && nd)
 #pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      double mx = use ? x[v] : -1.0e308, mn = use ? x[v] : 1.0e308;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
-        mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+      for (int v = 0; v < 8; ++v) {
+        run_max[v] = fmax(run_max[v], x[v]);
+        run_min[v] = fmin(run_min[v], x[v]);
       }
-      if (lane == 0) {
-        s_red[TE * 8 + v * 8 + warp] = mx;
-        s_red[TE * 8 + 64 + v * 8 + warp] = mn;
-      }
-    }
   }
   bool neg = false;
   if (limit) {
@@ -260,22 +253,47 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
 #pragma unroll
     for (int v = 0; v < 8; ++v)
       if (v % GS == node) u_avg[e * 8 + v] = avg[v];
-  if (need_global) {
+  if (NEEDG && need_global) {
     __syncthreads();
     if (tid < 8) {
       double sacc = 0.0;
       for (int q = 0; q < ne; ++q) sacc = sacc + s_red[q * 8 + tid];
       partial_out[tid] = sacc;
-      double a = s_red[TE * 8 + tid * 8], b = s_red[TE * 8 + 64 + tid * 8];
-      for (int w2 = 1; w2 < PP_NT / 32; ++w2) {
-        a = fmax(a, s_red[TE * 8 + tid * 8 + w2]);
-        b = fmin(b, s_red[TE * 8 + 64 + tid * 8 + w2]);
-      }
-      atomicMax(&ctrl->umax_bits[tid], ord_enc(a));
-      atomicMin(&ctrl->umin_bits[tid], ord_enc(b));
     }
     __syncthreads();  // s_red is reused by the next chunk
   }
+}
+
+// the CTA's running max/min of the interior node values -> ctrl->umax_bits/umin_bits
+// (max and min are exact, so the order of the reduction does not matter); resets the running values
+__device__ __forceinline__ void flush_minmax(double* run_max, double* run_min, double* s_red, Ctrl* ctrl) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    double mx = run_max[v], mn = run_min[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+      mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+    }
+    if (lane == 0) {
+      s_red[v * 8 + warp] = mx;
+      s_red[64 + v * 8 + warp] = mn;
+    }
+    run_max[v] = -1.0e308;
+    run_min[v] = 1.0e308;
+  }
+  __syncthreads();
+  if (tid < 8) {
+    double a = s_red[tid * 8], b = s_red[64 + tid * 8];
+    for (int w2 = 1; w2 < PP_NT / 32; ++w2) {
+      a = fmax(a, s_red[tid * 8 + w2]);
+      b = fmin(b, s_red[64 + tid * 8 + w2]);
+    }
+    if (a > -1.0e308) atomicMax(&ctrl->umax_bits[tid], ord_enc(a));
+    if (b < 1.0e308) atomicMin(&ctrl->umin_bits[tid], ord_enc(b));
+  }
+  __syncthreads();
 }
 
 template <int P>
@@ -284,9 +302,10 @@ __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s
   for (int it = threadIdx.x; it < N2 * N2; it += PP_NT) s_A[it] = __ldg(A + it);
 }
 
-// one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once)
-template <int P>
-__global__ void __launch_bounds__(PP_NT, PP_MINB)
+// one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once).
+// NEEDG: the OEDG form (need_global), with the global sums and extrema.
+template <int P, bool NEEDG>
+__global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
     pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                       int gate, int apply_ldf, int need_global, int ent_offset,
                       double* __restrict__ partial_sum,  // [chunks][8]
@@ -300,26 +319,40 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
   if (threadIdx.x == 0) s_cnt = 0;
   if (apply_ldf) load_ldf<P>(g.ldfA, s_A);
   __syncthreads();
+  double run_max[8], run_min[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    run_max[v] = -1.0e308;
+    run_min[v] = 1.0e308;
+  }
   for (int c = blockIdx.x; c < nchunks; c += gridDim.x)
-    pp_avg_ldf_chunk<P>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset, partial_sum + (long long)c * 8,
-                        cell_ent_DG, cell_ent_FV, cell_ent_nan, limit, s_A, s_red, &s_cnt);
+    pp_avg_ldf_chunk<P, NEEDG>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
+                               partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit, s_A,
+                               s_red, &s_cnt, run_max, run_min);
   __syncthreads();
+  if (NEEDG && need_global) flush_minmax(run_max, run_min, s_red, ctrl);
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
 }
 
 // many instances: items = every member's chunks; slot = the stage state; `final` selects the
 // final-stage form (OEDG global reductions for instances that use OEDG); the other stages fuse
 // loop 3 (limit)
-template <int P>
-__global__ void __launch_bounds__(PP_NT, PP_MINB)
+template <int P, bool FINAL>
+__global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
-                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate) {
   using C = PPCfg<P>;
   __shared__ double s_A[C::N2 * C::N2];
   __shared__ double s_red[C::TE * 8 + 128];
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
   int loaded = -1;  // member whose LDF operator s_A holds
+  double run_max[8], run_min[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    run_max[v] = -1.0e308;
+    run_min[v] = 1.0e308;
+  }
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
     const InstDesc& d = insts[m];
@@ -331,10 +364,12 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
       loaded = m;
     }
     __syncthreads();
-    pp_avg_ldf_chunk<P>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, d.use_oedg && final, d.ent_offset,
-                        d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan, !final, s_A,
-                        s_red, &s_cnt);
+    const int need_global = FINAL && d.use_oedg;
+    pp_avg_ldf_chunk<P, FINAL>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global, d.ent_offset,
+                               d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan, !FINAL,
+                               s_A, s_red, &s_cnt, run_max, run_min);
     __syncthreads();
+    if (need_global) flush_minmax(run_max, run_min, s_red, d.ctrl);  // per item: members differ
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
 }
