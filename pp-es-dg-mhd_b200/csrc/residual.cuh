@@ -21,23 +21,36 @@ namespace mhd {
 // Tile (TX x TY elements), threads per CTA and the CTAs per SM the register budget is cut for.
 template <int P>
 struct ResCfg;
-// HW = warps that start phase 2 on the interface fluxes (the rest start on the node pairs, which
-// every warp then shares through a shared-memory work counter).
-#ifndef MHD_RES_HW1
-#define MHD_RES_HW1 3
+// MHD_RES_CFG<p> = TX, TY, NT, MINB, HW, where HW = warps that start phase 2 on the interface
+// fluxes (all warps then share the node pairs through a shared-memory work counter).  The values
+// below were chosen by timing on B200; a build may override them (-DMHD_RES_CFG3=...).
+#ifndef MHD_RES_CFG1
+#define MHD_RES_CFG1 8, 4, 128, 4, 3
 #endif
-#ifndef MHD_RES_HW2
-#define MHD_RES_HW2 2
+#ifndef MHD_RES_CFG2
+#define MHD_RES_CFG2 4, 4, 128, 4, 2
 #endif
-#ifndef MHD_RES_HW3
-#define MHD_RES_HW3 3
+#ifndef MHD_RES_CFG3
+#define MHD_RES_CFG3 4, 2, 128, 4, 3
 #endif
+struct ResParams {
+  int TX, TY, NT, MINB, HW;
+};
 template <>
-struct ResCfg<1> { static constexpr int TX = 8, TY = 4, NT = 128, MINB = 4, HW = MHD_RES_HW1; };
+struct ResCfg<1> {
+  static constexpr ResParams c{MHD_RES_CFG1};
+  static constexpr int TX = c.TX, TY = c.TY, NT = c.NT, MINB = c.MINB, HW = c.HW;
+};
 template <>
-struct ResCfg<2> { static constexpr int TX = 4, TY = 4, NT = 128, MINB = 4, HW = MHD_RES_HW2; };
+struct ResCfg<2> {
+  static constexpr ResParams c{MHD_RES_CFG2};
+  static constexpr int TX = c.TX, TY = c.TY, NT = c.NT, MINB = c.MINB, HW = c.HW;
+};
 template <>
-struct ResCfg<3> { static constexpr int TX = 4, TY = 2, NT = 128, MINB = 4, HW = MHD_RES_HW3; };
+struct ResCfg<3> {
+  static constexpr ResParams c{MHD_RES_CFG3};
+  static constexpr int TX = c.TX, TY = c.TY, NT = c.NT, MINB = c.MINB, HW = c.HW;
+};
 
 template <int P>
 struct ResLayout {
