@@ -118,5 +118,39 @@ module mhd_gpu_bind
       integer(c_int), value :: check_every
       type(mhd_gpu_status), intent(out) :: st
     end function
+
+    ! ---- many instances advanced together (no reference counterpart) ----
+    integer(c_int) function mhd_batch_create(b) bind(C, name="mhd_batch_create")
+      import :: c_int, c_ptr
+      type(c_ptr), intent(out) :: b
+    end function
+
+    integer(c_int) function mhd_batch_destroy(b) bind(C, name="mhd_batch_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: b
+    end function
+
+    integer(c_int) function mhd_batch_add(b, h) bind(C, name="mhd_batch_add")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: b, h
+    end function
+
+    integer(c_int) function mhd_batch_remove(b, h) bind(C, name="mhd_batch_remove")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: b, h
+    end function
+
+    integer(c_int) function mhd_batch_advance(b, tries, n_active) bind(C, name="mhd_batch_advance")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: b
+      integer(c_int), value :: tries
+      integer(c_int), intent(out) :: n_active
+    end function
+
+    integer(c_int) function mhd_batch_member_status(b, h, st) bind(C, name="mhd_batch_member_status")
+      import :: c_int, c_ptr, mhd_gpu_status
+      type(c_ptr), value :: b, h
+      type(mhd_gpu_status), intent(out) :: st
+    end function
   end interface
 end module mhd_gpu_bind
