@@ -118,6 +118,31 @@ int mhd_gpu_download_ut(mhd_gpu_t *h, int stage, double *ut);
 /* u_avg (DG_solver.f90:11), the input of save_tecbin_finite_volume (io.f90:4) */
 int mhd_gpu_download_avg(mhd_gpu_t *h, double *u_avg);
 
+/* The cell-average output of save_tecbin_finite_volume (io.f90:75-86): MHD_con2pri
+ * (MHD_PDE.f90:44-56) of every interior u_avg, rounded to single precision, in the reference's
+ * buffer_var(nx+1, ny, 8) layout (Fortran order; the column nx+1, which the reference leaves
+ * unset, is zero), and the per-variable min/max of the rounded values (var_min, var_max: 8 each,
+ * may be NULL).  The Tecplot file itself is written by the host, as before. */
+int mhd_gpu_download_avg_primitive(mhd_gpu_t *h, float *buffer_var, double *var_min, double *var_max);
+
+/* ---- initial state on the device ---------------------------------------------------------- */
+
+/* init_by_fun_pri (problems.f90:25-51) for the set-ups of the package's problems module,
+ * evaluated at the GLL nodes on the GPU into slot 0 (u_con); the ghost ring is set to NaN.
+ * params (may be NULL / nparams 0 for the defaults):
+ *   MHD_IC_OT2PI, MHD_IC_OT_UNIT, MHD_IC_ROTOR, MHD_IC_ALFVEN: {amp}            (default 1)
+ *   MHD_IC_VORTEX: {kappa, mu, p_inf, bulk_vx, bulk_vy}                         (default 1,1,1,1,1)
+ *   MHD_IC_BLAST:  {centre_x, centre_y}                                         (default 0,0)
+ * Rotor: problems.f90:170-199; OT on [0,1]^2: :155-168; blast: :201-218; smooth Alfven: :74-98;
+ * OT on [0,2pi]^2 and the vortex are not in the reference (see the problems module). */
+#define MHD_IC_OT2PI 0
+#define MHD_IC_OT_UNIT 1
+#define MHD_IC_VORTEX 2
+#define MHD_IC_BLAST 3
+#define MHD_IC_ROTOR 4
+#define MHD_IC_ALFVEN 5
+int mhd_gpu_init_problem(mhd_gpu_t *h, int problem, const double *params, int nparams);
+
 /* ---- the reference's per-call interface -------------------------------------------------- */
 
 /* BC_handle(u_con or uRK_con(:,s), ...) (drive.f90:68,71,277,291) */

@@ -158,6 +158,22 @@ class DGSolver:
         return C.cast(p, C.c_void_p).value
 
     # -------------------------------------------------------------------------- reference calls
+    def init_problem(self, prob):
+        """the initial state of a problems-module set-up, evaluated on the GPU into slot 0"""
+        pid, params = prob.device_ic()
+        arr = (C.c_double * max(1, len(params)))(*params)
+        _check("mhd_gpu_init_problem", self.lib.mhd_gpu_init_problem(self.h, pid, arr, len(params)))
+
+    def download_avg_primitive(self):
+        """(buffer_var(nx+1, ny, 8) float32 Fortran order, var_min(8), var_max(8)) as
+        save_tecbin_finite_volume forms them from u_avg"""
+        buf = np.empty((self.nx + 1, self.ny, 8), dtype=np.float32, order="F")
+        vmin, vmax = np.empty(8), np.empty(8)
+        _check("mhd_gpu_download_avg_primitive",
+               self.lib.mhd_gpu_download_avg_primitive(self.h, buf.ctypes.data_as(C.POINTER(C.c_float)), _p(vmin),
+                                                       _p(vmax)))
+        return buf, vmin, vmax
+
     def apply_bc(self, slot):
         _check("mhd_gpu_apply_bc", self.lib.mhd_gpu_apply_bc(self.h, slot))
 

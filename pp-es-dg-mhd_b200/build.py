@@ -14,8 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmhd_gpu.so")
 SOURCES = ["mhd_gpu.cu", "tables.cpp"]
-DEPS = SOURCES + ["common.cuh", "residual.cuh", "post.cuh", "misc.cuh", "tables.h", "batch_impl.cuh",
-                  "server_impl.cuh"]
+DEPS = SOURCES + ["common.cuh", "residual.cuh", "post.cuh", "misc.cuh", "setup.cuh", "tables.h",
+                  "batch_impl.cuh", "server_impl.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",

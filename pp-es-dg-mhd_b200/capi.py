@@ -14,6 +14,8 @@ MHD_FLAG_NEG_AVG = 1
 MHD_FLAG_PP_RELIMIT = 2
 MHD_FLAG_DT_COLLAPSE = 4
 MHD_FLAG_INIT_NEG_AVG = 8
+
+IC_OT2PI, IC_OT_UNIT, IC_VORTEX, IC_BLAST, IC_ROTOR, IC_ALFVEN = range(6)
 MHD_ERR_INVALID = -1
 MHD_ERR_UNSUPPORTED = -2
 MHD_ERR_CUDA = -3
@@ -113,6 +115,8 @@ SIGNATURES = {
     "mhd_server_results": (C.c_int, [_vp, C.POINTER(RequestResult), C.c_int, C.POINTER(C.c_int)]),
     "mhd_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
     "mhd_server_destroy": (C.c_int, [_vp]),
+    "mhd_gpu_download_avg_primitive": (C.c_int, [_vp, C.POINTER(C.c_float), _dp, _dp]),
+    "mhd_gpu_init_problem": (C.c_int, [_vp, C.c_int, _dp, C.c_int]),
     "mhd_gpu_semidiscretize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                  C.c_double, _vp, _vp, _dp, _vp]),
 }

@@ -8,6 +8,7 @@
 // with 128-bit loads.  The time derivative ut has the same per-element blocks without the ghost
 // ring: ut[ j-1 ][ i-1 ][ var ][ node ].
 #pragma once
+#include <cstring>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -106,6 +107,14 @@ __device__ __forceinline__ unsigned long long ord_enc(double x) {
 __device__ __forceinline__ double ord_dec(unsigned long long e) {
   return (e & 0x8000000000000000ULL) ? __longlong_as_double((long long)(e & 0x7FFFFFFFFFFFFFFFULL))
                                      : __longlong_as_double((long long)~e);
+}
+
+// the same decoding on the host (for reduction results copied back)
+inline double ord_dec_host(unsigned long long e) {
+  const unsigned long long b = (e & 0x8000000000000000ULL) ? (e & 0x7FFFFFFFFFFFFFFFULL) : ~e;
+  double d;
+  std::memcpy(&d, &b, sizeof(d));
+  return d;
 }
 
 __device__ __forceinline__ bool gate_open(const Ctrl* c, int gate) {

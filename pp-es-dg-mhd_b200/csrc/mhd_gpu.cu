@@ -20,6 +20,7 @@
 #include "misc.cuh"
 #include "post.cuh"
 #include "residual.cuh"
+#include "setup.cuh"
 #include "tables.h"
 
 using namespace mhd;
@@ -583,6 +584,72 @@ int mhd_gpu_download_avg(mhd_gpu_t* h, double* u_avg) {
   if (!u_avg) return MHD_ERR_INVALID;
   CK(cudaMemcpyAsync(u_avg, h->u_avg, sizeof(double) * 8 * (size_t)(h->nx + 2) * (h->ny + 2),
                      cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+
+int mhd_gpu_download_avg_primitive(mhd_gpu_t* h, float* buffer_var, double* var_min, double* var_max) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!buffer_var) return MHD_ERR_INVALID;
+  const long long cells = (long long)(h->nx + 1) * h->ny;
+  float* dout = reinterpret_cast<float*>(h->staging);  // 8*cells floats fit the staging buffer
+  unsigned long long* mm = reinterpret_cast<unsigned long long*>(h->partial);  // 16 words of scratch
+  unsigned long long init[16];
+  for (int v = 0; v < 8; ++v) {
+    init[v] = ~0ULL;
+    init[8 + v] = 0ULL;
+  }
+  CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+  avg_primitive_kernel<<<grid1d(cells, 256), 256, 0, h->stream>>>(h->u_avg, h->geo, dout, mm);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(buffer_var, dout, sizeof(float) * 8 * cells, cudaMemcpyDeviceToHost, h->stream));
+  unsigned long long got[16];
+  CK(cudaMemcpyAsync(got, mm, sizeof(got), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int v = 0; v < 8; ++v) {
+    if (var_min) var_min[v] = ord_dec_host(got[v]);
+    if (var_max) var_max[v] = ord_dec_host(got[8 + v]);
+  }
+  return MHD_OK;
+}
+
+int mhd_gpu_init_problem(mhd_gpu_t* h, int problem, const double* params, int nparams) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (problem < MHD_IC_OT2PI || problem > MHD_IC_ALFVEN || nparams < 0 || (nparams > 0 && !params))
+    return MHD_ERR_INVALID;
+  ProblemParams pp{};
+  pp.id = problem;
+  pp.amp = 1.0;
+  pp.kappa = pp.mu = pp.p_inf = pp.bx0 = pp.by0 = 1.0;
+  pp.cx = pp.cy = 0.0;
+  auto arg = [&](int k, double dflt) { return k < nparams ? params[k] : dflt; };
+  switch (problem) {
+    case MHD_IC_VORTEX:
+      pp.kappa = arg(0, 1.0);
+      pp.mu = arg(1, 1.0);
+      pp.p_inf = arg(2, 1.0);
+      pp.bx0 = arg(3, 1.0);
+      pp.by0 = arg(4, 1.0);
+      if (nparams > 5) return MHD_ERR_INVALID;
+      break;
+    case MHD_IC_BLAST:
+      pp.cx = arg(0, 0.0);
+      pp.cy = arg(1, 0.0);
+      if (nparams > 2) return MHD_ERR_INVALID;
+      break;
+    default:
+      pp.amp = arg(0, 1.0);
+      if (nparams > 1) return MHD_ERR_INVALID;
+  }
+  const long long n = (long long)(h->nx + 2) * (h->ny + 2) * h->nn;
+  switch (h->p) {
+    case 1: init_problem_kernel<1><<<grid1d(n, 256), 256, 0, h->stream>>>(h->u[0], h->geo, pp, h->left, h->bottom); break;
+    case 2: init_problem_kernel<2><<<grid1d(n, 256), 256, 0, h->stream>>>(h->u[0], h->geo, pp, h->left, h->bottom); break;
+    default: init_problem_kernel<3><<<grid1d(n, 256), 256, 0, h->stream>>>(h->u[0], h->geo, pp, h->left, h->bottom); break;
+  }
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
   return MHD_OK;
 }

@@ -147,6 +147,19 @@ class Problem:
     params: dict = field(default_factory=dict)
     bc_state: object = None
 
+    def device_ic(self):
+        """(problem id, parameters) of mhd_gpu_init_problem for this set-up"""
+        ids = {"ot2pi": capi.IC_OT2PI, "ot_unit": capi.IC_OT_UNIT, "vortex": capi.IC_VORTEX,
+               "blast": capi.IC_BLAST, "rotor": capi.IC_ROTOR, "alfven": capi.IC_ALFVEN}
+        if self.name == "vortex":
+            kw = dict(kappa=1.0, mu=1.0, p_inf=1.0, bulk=(1.0, 1.0))
+            kw.update(self.params)
+            return ids["vortex"], [kw["kappa"], kw["mu"], kw["p_inf"], kw["bulk"][0], kw["bulk"][1]]
+        if self.name == "blast":
+            c = self.params.get("center", (0.0, 0.0))
+            return ids["blast"], [c[0], c[1]]
+        return ids[self.name], [self.params.get("amp", 1.0)]
+
     def initial_state(self, nx, ny, p):
         """u(8, p+1, p+1, nx+2, ny+2) Fortran order, interior from the IC, ghost ring NaN."""
         xx, yy = node_coords(nx, ny, p, self.domain)

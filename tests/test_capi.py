@@ -76,3 +76,15 @@ def test_struct_layouts_match_the_header(pkg, tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_set_up_entry_points_reject_bad_arguments(pkg):
+    lib = pkg.capi.load()
+    assert lib.mhd_gpu_init_problem(None, 0, None, 0) == pkg.capi.MHD_ERR_INVALID
+    assert lib.mhd_gpu_download_avg_primitive(None, None, None, None) == pkg.capi.MHD_ERR_INVALID
+
+
+def test_every_problem_has_a_device_initial_state(pkg):
+    for name in ("ot2pi", "ot_unit", "vortex", "blast", "rotor", "alfven"):
+        pid, params = pkg.problems.make(name).device_ic()
+        assert 0 <= pid <= 5 and len(params) in (1, 2, 5)
