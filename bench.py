@@ -287,6 +287,72 @@ SERVE_STREAMS = {"spec_N32-512": dict(n_req=64, rate=200.0, n_hi=512, t_scale=0.
                  "small_N32-96": dict(n_req=128, rate=2000.0, n_hi=96, t_scale=0.5)}
 
 
+def batched_leg(pkg, n_runs=512, steps=4, seed=11, n_lo=32, n_hi=256, sample=8):
+    """the batched configuration of the scope table: n_runs independent runs (N ~ U[n_lo, n_hi],
+    p ~ U{1,2,3}, IC in {OT, rotor}, amplitude ~ U[0.5, 1.5], gamma in {5/3, 1.4}), initial states
+    evaluated on the device.  Timed with CUDA events: `steps` steps of every run one after another
+    (each run's own CUDA graph), then the same from the same initial states as one batch (shared
+    persistent launches, one CUDA graph per try); one untimed step and the graph captures come
+    first in both.  `identical` counts sampled runs whose final state is bitwise the same both ways."""
+    import torch
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n_runs):
+        name = ["ot2pi", "rotor"][int(rng.integers(0, 2))]
+        specs.append(dict(name=name, n=int(rng.integers(n_lo, n_hi + 1)), p=int(rng.integers(1, 4)),
+                          amp=float(rng.uniform(0.5, 1.5)), gamma=[5.0 / 3.0, 1.4][int(rng.integers(0, 2))]))
+    probs = [pkg.problems.make(sp["name"], gamma=sp["gamma"], amp=sp["amp"]) for sp in specs]
+    runs = [pkg.DGSolver.for_problem(pr, sp["n"], sp["n"], sp["p"]) for pr, sp in zip(probs, specs)]
+    dofs = sum(8 * sp["n"] ** 2 * (sp["p"] + 1) ** 2 for sp in specs)
+
+    def start():  # initial state, then one untimed step each (loads kernels, builds each run's graph)
+        for r, pr in zip(runs, probs):
+            r.init_problem(pr)
+            r.solve_begin(pr.final_T, pr.cfl)
+            r.advance(1)
+        torch.cuda.synchronize()
+
+    # the calls below return only when their work is done, so events recorded on the default stream
+    # just before and just after bracket it on the device
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start()
+    e0.record()
+    tries_solo = 0
+    for r in runs:
+        st = r.advance(steps, check_every=steps)
+        tries_solo += st["steps"] + st["retries"]
+    e1.record()
+    torch.cuda.synchronize()
+    ms_solo = e0.elapsed_time(e1)
+    ref = [runs[i].download_state(0) for i in range(sample)]
+    start()
+    b = pkg.Batch()
+    for r in runs:
+        b.add(r)
+    b.advance(0)  # uploads the tables and captures the batch graph, untimed
+    torch.cuda.synchronize()
+    e0.record()
+    b.advance(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    sts = [b.status(r) for r in runs]
+    for r in list(runs):
+        b.remove(r)
+    b.close()
+    same = sum(int(np.array_equal(runs[i].download_state(0), ref[i], equal_nan=True)) for i in range(sample))
+    for r in runs:
+        r.close()
+    stage_updates = 3 * dofs * steps
+    return {"runs": n_runs, "dofs": dofs, "steps": steps,
+            "batched": {"ms": ms_b, "dof_stage_per_s": stage_updates / (ms_b * 1e-3)},
+            "one_after_another": {"ms": ms_solo, "dof_stage_per_s": stage_updates / (ms_solo * 1e-3)},
+            "speedup": ms_solo / ms_b, "identical": f"{same}/{sample}",
+            "retries": int(sum(s["retries"] for s in sts)),
+            "config": f"{n_runs} runs, seed {seed}, N ~ U[{n_lo},{n_hi}], p ~ U{{1,2,3}}, IC in {{OT, rotor}}, "
+                      f"amp ~ U[0.5,1.5], gamma in {{5/3, 1.4}}, {steps} SSP-RK3 steps each"}
+
+
 # ------------------------------------------------------------------------------ GPU leg
 def run_ours(args):
     import torch
@@ -412,6 +478,8 @@ def run_ours(args):
         }
         if e2e:
             line["e2e"] = e2e
+        if not args.no_batched and ws == 1:
+            line["batched"] = batched_leg(pkg)
         if not args.no_serve and ws == 1:
             line["served"] = {k: serve_leg(pkg, **kw) for k, kw in SERVE_STREAMS.items()}
         if not args.no_cpu and ws == 1:
@@ -434,6 +502,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     args = ap.parse_args()
     if args.impl == "reference":

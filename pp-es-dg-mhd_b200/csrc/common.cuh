@@ -99,6 +99,36 @@ __device__ __forceinline__ int batch_member(const int* __restrict__ pref, int n,
   return lo;
 }
 
+// The items a CTA of a batched kernel takes: one contiguous share [b*nw/G, (b+1)*nw/G) of the
+// group's nw items (CTA b of G), visited in order.  The member is found by binary search once and
+// then walked forward, so consecutive items of one member reuse its descriptor (and whatever the
+// kernel staged for it), and neighbouring tiles of a member are processed close in time.
+struct BatchWalk {
+  const int* pref;
+  int w, last, m, mstart, mend;
+  __device__ __forceinline__ BatchWalk(const int* __restrict__ pref_, int n, int nw) : pref(pref_) {
+    const long long b = blockIdx.x, G = gridDim.x;
+    w = (int)(b * nw / G);
+    last = (int)((b + 1) * nw / G);
+    m = mstart = mend = 0;
+    if (w < last) {
+      m = batch_member(pref, n, w);
+      mstart = __ldg(pref + m);
+      mend = __ldg(pref + m + 1);
+    }
+  }
+  __device__ __forceinline__ bool more() const { return w < last; }
+  __device__ __forceinline__ int local() const { return w - mstart; }
+  __device__ __forceinline__ void next() {
+    ++w;
+    while (w < last && w >= mend) {
+      ++m;
+      mstart = mend;
+      mend = __ldg(pref + m + 1);
+    }
+  }
+};
+
 // ---- order-preserving encodings of doubles for atomicMax / atomicMin --------------------------
 __device__ __forceinline__ unsigned long long ord_enc(double x) {
   long long b = __double_as_longlong(x);

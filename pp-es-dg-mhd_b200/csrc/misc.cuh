@@ -60,8 +60,8 @@ __global__ void __launch_bounds__(256) bc_batched(const InstDesc* __restrict__ i
                                                   const int* __restrict__ nwork, const int* __restrict__ ninst,
                                                   int slot, int gate) {
   const int nw = *nwork, n = *ninst;
-  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, chunk = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
     bc_value<P>(d.u[slot], d.g, (long long)chunk * 256 + threadIdx.x);
@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(256) combine_batched(const InstDesc* __restric
                                                        const int* __restrict__ nwork, const int* __restrict__ ninst,
                                                        int stage, int gate) {
   const int nw = *nwork, n = *ninst;
-  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, chunk = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
     combine_value<EB>(d.u[0], d.u[1], d.u[2], d.u[3], d.u[4], d.ut[1], d.ut[2], d.ut[3], d.ut[4], d.ut[5],

@@ -353,8 +353,8 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     run_max[v] = -1.0e308;
     run_min[v] = 1.0e308;
   }
-  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), chunk = w - __ldg(pref + m);
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, chunk = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
     if (threadIdx.x == 0) s_cnt = 0;
@@ -576,8 +576,8 @@ __global__ void __launch_bounds__(256, 2)
     pp_sigsum_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   const int nw = *nwork, n = *ninst;
-  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, local = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
     const int ntx = (d.g.nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX;
@@ -705,8 +705,8 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
   __shared__ double s_ent[PPCfg<P>::TE];
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
-  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, local = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
     if (threadIdx.x == 0) s_cnt = 0;

@@ -436,8 +436,8 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate) {
   extern __shared__ __align__(16) double sm[];
   const int nw = *nwork, n = *ninst;
-  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
-    const int m = batch_member(pref, n, w), local = w - __ldg(pref + m);
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, local = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
     const int ntx = (d.g.nx + ResCfg<P>::TX - 1) / ResCfg<P>::TX;
