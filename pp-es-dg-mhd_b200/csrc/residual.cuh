@@ -79,7 +79,8 @@ struct ResLayout {
   static constexpr int O_FY = O_FX + NFX * FW;
   static constexpr int O_PAIR = O_FY + NFY * FW;
   static constexpr int O_SIG = O_PAIR + TE * NPAIR * 8;
-  static constexpr int O_RED = O_SIG + TE * 2 * NN;
+  static constexpr int O_PT = O_SIG + TE * 2 * NN;  // total pressure p + |B|^2/2 per node
+  static constexpr int O_RED = O_PT + TE * NN;
   static constexpr int TOTAL = O_RED + 32;  // O_RED + 16 doubles also hold the pair work counter
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
 };
@@ -117,6 +118,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   double* s_fy = sm + L::O_FY;
   double* s_pair = sm + L::O_PAIR;
   double* s_sig = sm + L::O_SIG;
+  double* s_pt = sm + L::O_PT;
   double* s_red = sm + L::O_RED;
   int* s_next = reinterpret_cast<int*>(s_red + 16);  // next node-pair chunk of phase 2
 
@@ -181,6 +183,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
     pr[6 * NN] = w[6];
     pr[7 * NN] = 0.5 * w[0] / pf;
     const double cs = gamma * pf * ir, ss = cs + bsq * ir, coef = 4.0 * cs * ir;
+    s_pt[e * NN + q] = pf + 0.5 * bsq;
     s_sig[e * 2 * NN + q] = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
     s_sig[e * 2 * NN + NN + q] = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
   }
@@ -287,15 +290,11 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       double w[8];
 #pragma unroll
       for (int v = 0; v < 8; ++v) w[v] = cw[v * NN];
-      // node flux F, G and Godunov-Powell coefficients (DG_solver.f90:749-799)
-      const double ir = 1.0 / w[0];
-      const double vx = ir * w[1], vy = ir * w[2], vz = ir * w[3];
+      // node flux F, G and Godunov-Powell coefficients (DG_solver.f90:749-799); the velocities
+      // and the total pressure are the node's phase-1 values
+      const double vx = pb[1 * NN + q], vy = pb[2 * NN + q], vz = pb[3 * NN + q];
       const double bx = w[4], by = w[5], bz = w[6];
-      const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
-      const double bsq = bx * bx + by * by + bz * bz;
-      const double pm = 0.5 * bsq;
-      const double pf = fmax((gamma - 1.0) * (w[7] - (ek + pm)), PP_EPS);
-      const double pt = pf + pm;
+      const double pt = s_pt[e * NN + q];
       const double bu = bx * vx + by * vy + bz * vz;
       const double ex = by * vz - bz * vy, ey = bz * vx - bx * vz, ez = bx * vy - by * vx;
       double F[8], G[8], GP[8];
