@@ -48,6 +48,9 @@ typedef struct mhd_gpu mhd_gpu_t;
 #define MHD_BC_EXTRAPOLATE 1      /* BC_YeeSjogreen  problems.f90:386-423 (outflow) */
 #define MHD_BC_FIXED 2            /* BC_rotor        problems.f90:597-654 (bc_state8 = conserved state) */
 #define MHD_BC_XEXTRAP_YPER 3     /* BC_BrioWu       problems.f90:350-384 */
+#define MHD_BC_CLOUD_SHOCK 4      /* BC_cloud_shock  problems.f90:425-472 (bc_state8 = right inflow state) */
+#define MHD_BC_JET 5              /* BC_jet1_cell_ext problems.f90:474-595 (bc_state8 = nozzle state,
+                                     below the first nx/10 elements of the bottom side) */
 
 /* status of the device-resident driver (the scalars solve_execute keeps, drive.f90:39-48) */
 typedef struct mhd_gpu_status {
@@ -68,7 +71,8 @@ typedef struct mhd_gpu_status {
 
 /* init_DG_solver(nx,ny,px,py,rknstg,l,r,b,t) (DG_solver.f90:47-107) + set_gamma (MHD_PDE.f90:5)
  * + the choice of BC_handle (drive.f90:25).  Allocates every device array NaN-filled
- * (DG_solver.f90:56,68-85).  bc_state8 is required for MHD_BC_FIXED, else may be NULL. */
+ * (DG_solver.f90:56,68-85).  bc_state8 is required for MHD_BC_FIXED, MHD_BC_CLOUD_SHOCK and
+ * MHD_BC_JET, else may be NULL. */
 int mhd_gpu_create(int nx, int ny, int px, int py, int rknstg, double left, double right,
                    double bottom, double top, double gamma, int bc_kind, const double *bc_state8,
                    mhd_gpu_t **out);
@@ -141,6 +145,8 @@ int mhd_gpu_download_avg_primitive(mhd_gpu_t *h, float *buffer_var, double *var_
 #define MHD_IC_BLAST 3
 #define MHD_IC_ROTOR 4
 #define MHD_IC_ALFVEN 5
+#define MHD_IC_CLOUD_SHOCK 6  /* cloud_shock_init_pri (problems.f90:220-247), no parameters */
+#define MHD_IC_JET 7          /* jet1_init_pri (problems.f90:249-257), no parameters */
 int mhd_gpu_init_problem(mhd_gpu_t *h, int problem, const double *params, int nparams);
 
 /* ---- the reference's per-call interface -------------------------------------------------- */

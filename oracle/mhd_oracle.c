@@ -805,6 +805,43 @@ void ora_apply_bc(ora_solver *s, double *u) {
         memcpy(EB(s, u, i, ny + 1), EB(s, u, i, 1), blk);
       }
       break;
+    case ORA_BC_CLOUD_SHOCK: /* problems.f90:449-471: copies, and the inflow state on the right */
+#pragma omp parallel for schedule(static)
+      for (int j = 1; j <= ny; ++j) {
+        memcpy(EB(s, u, 0, j), EB(s, u, 1, j), blk);
+        for (int q = 0; q < nq; ++q)
+          for (int v = 0; v < 8; ++v) EB(s, u, nx + 1, j)[v + 8 * q] = s->bc_state[v];
+      }
+#pragma omp parallel for schedule(static)
+      for (int i = 1; i <= nx; ++i) {
+        memcpy(EB(s, u, i, 0), EB(s, u, i, 1), blk);
+        memcpy(EB(s, u, i, ny + 1), EB(s, u, i, ny), blk);
+      }
+      break;
+    case ORA_BC_JET: /* problems.f90:502-593 */
+#pragma omp parallel for schedule(static)
+      for (int j = 1; j <= ny; ++j) {
+        /* left: mirror of element 1 in x (node k <- px-k), normal momentum and field negated */
+        for (int l = 0; l < s->nqy; ++l)
+          for (int k = 0; k < s->nqx; ++k)
+            for (int v = 0; v < 8; ++v) {
+              const double x = EB(s, u, 1, j)[NODE(s, v, s->px - k, l)];
+              EB(s, u, 0, j)[NODE(s, v, k, l)] = (v == 1 || v == 4) ? -x : x;
+            }
+        /* right: copy element nx */
+        memcpy(EB(s, u, nx + 1, j), EB(s, u, nx, j), blk);
+      }
+#pragma omp parallel for schedule(static)
+      for (int i = 1; i <= nx; ++i) {
+        if (i <= nx / 10) { /* the nozzle (the reference requires nx to be a multiple of 10) */
+          for (int q = 0; q < nq; ++q)
+            for (int v = 0; v < 8; ++v) EB(s, u, i, 0)[v + 8 * q] = s->bc_state[v];
+        } else {
+          memcpy(EB(s, u, i, 0), EB(s, u, i, 1), blk);
+        }
+        memcpy(EB(s, u, i, ny + 1), EB(s, u, i, ny), blk);
+      }
+      break;
     default:
       break;
   }

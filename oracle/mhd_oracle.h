@@ -42,7 +42,9 @@ enum {
   ORA_BC_PERIODIC = 0,      /* BC_periodic      problems.f90:312-348 */
   ORA_BC_EXTRAPOLATE = 1,   /* BC_YeeSjogreen   problems.f90:386-423 */
   ORA_BC_FIXED = 2,         /* BC_rotor pattern problems.f90:597-654 (state given) */
-  ORA_BC_XEXTRAP_YPER = 3   /* BC_BrioWu        problems.f90:350-384 */
+  ORA_BC_XEXTRAP_YPER = 3,  /* BC_BrioWu        problems.f90:350-384 */
+  ORA_BC_CLOUD_SHOCK = 4,   /* BC_cloud_shock   problems.f90:425-472 (state = right inflow) */
+  ORA_BC_JET = 5            /* BC_jet1_cell_ext problems.f90:474-595 (state = bottom nozzle) */
 };
 
 /* status codes returned by ora_solve */

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import build_oracle
 
-BC_PERIODIC, BC_EXTRAPOLATE, BC_FIXED, BC_XEXTRAP_YPER = 0, 1, 2, 3
+BC_PERIODIC, BC_EXTRAPOLATE, BC_FIXED, BC_XEXTRAP_YPER, BC_CLOUD_SHOCK, BC_JET = 0, 1, 2, 3, 4, 5
 
 _libs = {}
 _dp = C.POINTER(C.c_double)

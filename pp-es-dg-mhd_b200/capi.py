@@ -15,14 +15,14 @@ MHD_FLAG_PP_RELIMIT = 2
 MHD_FLAG_DT_COLLAPSE = 4
 MHD_FLAG_INIT_NEG_AVG = 8
 
-IC_OT2PI, IC_OT_UNIT, IC_VORTEX, IC_BLAST, IC_ROTOR, IC_ALFVEN = range(6)
+IC_OT2PI, IC_OT_UNIT, IC_VORTEX, IC_BLAST, IC_ROTOR, IC_ALFVEN, IC_CLOUD_SHOCK, IC_JET = range(8)
 MHD_ERR_INVALID = -1
 MHD_ERR_UNSUPPORTED = -2
 MHD_ERR_CUDA = -3
 MHD_ERR_NO_DEVICE = -4
 MHD_ERR_STATE = -5
 
-BC_PERIODIC, BC_EXTRAPOLATE, BC_FIXED, BC_XEXTRAP_YPER = 0, 1, 2, 3
+BC_PERIODIC, BC_EXTRAPOLATE, BC_FIXED, BC_XEXTRAP_YPER, BC_CLOUD_SHOCK, BC_JET = 0, 1, 2, 3, 4, 5
 
 
 class Status(C.Structure):

@@ -372,8 +372,9 @@ int create_instance(int nx, int ny, int px, int py, int rknstg, double left, dou
   if (nx < 2 || ny < 2 || !(right > left) || !(top > bottom) || !(gamma > 1.0)) return MHD_ERR_INVALID;
   if (px != py || px < 1 || px > MAXP) return MHD_ERR_UNSUPPORTED;
   if (!(rknstg == 1 || rknstg == 2 || rknstg == 3 || rknstg == 5)) return MHD_ERR_UNSUPPORTED;
-  if (bc_kind < 0 || bc_kind > 3) return MHD_ERR_INVALID;
-  if (bc_kind == MHD_BC_FIXED && !bc_state8) return MHD_ERR_INVALID;
+  if (bc_kind < 0 || bc_kind > 5) return MHD_ERR_INVALID;
+  if ((bc_kind == MHD_BC_FIXED || bc_kind == MHD_BC_CLOUD_SHOCK || bc_kind == MHD_BC_JET) && !bc_state8)
+    return MHD_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MHD_ERR_NO_DEVICE;
   mhd_gpu* h = new (std::nothrow) mhd_gpu;
@@ -617,7 +618,7 @@ int mhd_gpu_download_avg_primitive(mhd_gpu_t* h, float* buffer_var, double* var_
 int mhd_gpu_init_problem(mhd_gpu_t* h, int problem, const double* params, int nparams) {
   int rc = enter(h);
   if (rc) return rc;
-  if (problem < MHD_IC_OT2PI || problem > MHD_IC_ALFVEN || nparams < 0 || (nparams > 0 && !params))
+  if (problem < MHD_IC_OT2PI || problem > MHD_IC_JET || nparams < 0 || (nparams > 0 && !params))
     return MHD_ERR_INVALID;
   ProblemParams pp{};
   pp.id = problem;

@@ -5,7 +5,9 @@
 
 namespace mhd {
 
-enum BcKind : int { BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_FIXED = 2, BC_XEXTRAP_YPER = 3 };
+enum BcKind : int {
+  BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_FIXED = 2, BC_XEXTRAP_YPER = 3, BC_CLOUD_SHOCK = 4, BC_JET = 5
+};
 
 // Ghost-ring fill (problems.f90:312-423,597-654).  One thread per ghost value; corners untouched.
 template <int P>
@@ -25,6 +27,30 @@ __device__ __forceinline__ void bc_value(double* __restrict__ u, const Geo& g, l
   else { i = 1 + ge - 2 * ny - nx; j = ny + 1; xside = false; }
   const long long dst = ((long long)j * NXG + i) * EB + vi;
   int kind = g.bc_kind;
+  if (kind == BC_CLOUD_SHOCK || kind == BC_JET) {
+    // BC_cloud_shock (problems.f90:449-471): element copies, inflow state on the right.
+    // BC_jet1_cell_ext (problems.f90:502-593): mirror of element 1 on the left (k <- n-1-k, normal
+    // momentum and field negated), copies elsewhere, the nozzle state below i <= nx/10.
+    double sign = 1.0;
+    if (kind == BC_CLOUD_SHOCK && i == nx + 1) {
+      u[dst] = g.bc_state[v];
+      return;
+    }
+    if (kind == BC_JET && j == 0 && i <= nx / 10) {
+      u[dst] = g.bc_state[v];
+      return;
+    }
+    si = (i == 0) ? 1 : (i == nx + 1 ? nx : i);
+    sj = (j == 0) ? 1 : (j == ny + 1 ? ny : j);
+    sq = q;
+    if (kind == BC_JET && i == 0) {
+      sq = (N - 1 - k) + N * l;
+      if (v == 1 || v == 4) sign = -1.0;
+    }
+    const double x = u[((long long)sj * NXG + si) * EB + v * NN + sq];
+    u[dst] = sign < 0.0 ? -x : x;
+    return;
+  }
   if (kind == BC_XEXTRAP_YPER) kind = xside ? BC_EXTRAPOLATE : BC_PERIODIC;
   if (kind == BC_FIXED) {
     u[dst] = g.bc_state[v];

@@ -12,7 +12,9 @@
 
 namespace mhd {
 
-enum ProblemId : int { IC_OT2PI = 0, IC_OT_UNIT = 1, IC_VORTEX = 2, IC_BLAST = 3, IC_ROTOR = 4, IC_ALFVEN = 5 };
+enum ProblemId : int {
+  IC_OT2PI = 0, IC_OT_UNIT = 1, IC_VORTEX = 2, IC_BLAST = 3, IC_ROTOR = 4, IC_ALFVEN = 5, IC_CLOUD_SHOCK = 6, IC_JET = 7
+};
 
 struct ProblemParams {
   int id;
@@ -75,6 +77,25 @@ __device__ __forceinline__ void problem_pri(const ProblemParams& pp, double x, d
       w[7] = 1.0;
       break;
     }
+    case IC_CLOUD_SHOCK:  // cloud_shock_init_pri (problems.f90:220-247), "original formulation"
+      if (x < 0.6) {
+        w[0] = 3.86859;
+        w[5] = 2.1826182;
+        w[6] = -2.1826182;
+        w[7] = 167.345;
+      } else {
+        w[0] = ((x - 0.8) * (x - 0.8) + (y - 0.5) * (y - 0.5) <= 0.15 * 0.15) ? 10.0 : 1.0;
+        w[1] = -11.2536;
+        w[5] = 0.56418958;
+        w[6] = 0.56418958;
+        w[7] = 1.0;
+      }
+      break;
+    case IC_JET:  // jet1_init_pri (problems.f90:249-257)
+      w[0] = 0.1 * gamma;
+      w[5] = sqrt(200.0);
+      w[7] = 1.0;
+      break;
     default: {  // smooth_alfven_init_fun (problems.f90:74-98)
       const double al = IC_PI / 6.0, ca = cos(al), sa = sin(al);
       const double xp = x * ca + y * sa;

@@ -16,6 +16,8 @@ Problems
   rotor     the reference's Rotor_init_pri (problems.f90:170-199) with BC_rotor fixed ghosts
             (problems.f90:597-654), gamma = 1.4.
   alfven    the reference's smooth_alfven_init_fun (problems.f90:74-98), periodic.
+  cloud_shock  cloud_shock_init_pri (problems.f90:220-247) with BC_cloud_shock (:425-472).
+  jet       jet1_init_pri (problems.f90:249-257) with BC_jet1_cell_ext (:474-595), gamma 1.4.
 An amplitude factor `amp` scales velocity and magnetic field perturbations (ot2pi, rotor).
 """
 import ctypes as C
@@ -125,6 +127,23 @@ def rotor_pri(x, y, gamma, amp=1.0):
     return np.stack([rho, vx, vy, z, z + amp * 5.0 / math.sqrt(4 * PI), z, z, z + 1.0])
 
 
+def cloud_shock_pri(x, y, gamma, amp=1.0):
+    """cloud_shock_init_pri (problems.f90:220-247), the reference's "original formulation" values"""
+    post = np.array([3.86859, 0.0, 0.0, 0.0, 0.0, 2.1826182, -2.1826182, 167.345])
+    pre = np.array([1.0, -11.2536, 0.0, 0.0, 0.0, 0.56418958, 0.56418958, 1.0])
+    left = x < 0.6
+    u = np.where(left[None], post.reshape((8,) + (1,) * x.ndim), pre.reshape((8,) + (1,) * x.ndim))
+    cloud = (~left) & ((x - 0.8) ** 2 + (y - 0.5) ** 2 <= 0.15 ** 2)
+    u[0] = np.where(cloud, 10.0, u[0])
+    return u
+
+
+def jet_pri(x, y, gamma, amp=1.0):
+    """jet1_init_pri (problems.f90:249-257): the ambient state"""
+    z = np.zeros_like(x)
+    return np.stack([z + 0.1 * gamma, z, z, z, z, z + math.sqrt(200.0), z, z + 1.0])
+
+
 def alfven_pri(x, y, gamma, amp=1.0):
     al = PI / 6.0
     xp = x * math.cos(al) + y * math.sin(al)
@@ -150,7 +169,8 @@ class Problem:
     def device_ic(self):
         """(problem id, parameters) of mhd_gpu_init_problem for this set-up"""
         ids = {"ot2pi": capi.IC_OT2PI, "ot_unit": capi.IC_OT_UNIT, "vortex": capi.IC_VORTEX,
-               "blast": capi.IC_BLAST, "rotor": capi.IC_ROTOR, "alfven": capi.IC_ALFVEN}
+               "blast": capi.IC_BLAST, "rotor": capi.IC_ROTOR, "alfven": capi.IC_ALFVEN,
+               "cloud_shock": capi.IC_CLOUD_SHOCK, "jet": capi.IC_JET}
         if self.name == "vortex":
             kw = dict(kappa=1.0, mu=1.0, p_inf=1.0, bulk=(1.0, 1.0))
             kw.update(self.params)
@@ -195,6 +215,15 @@ def make(name, gamma=None, amp=1.0, **kw):
         st = pri2con(np.array([1.0, 0.0, 0.0, 0.0, amp * 5.0 / math.sqrt(4 * PI), 0.0, 0.0, 1.0]), g)
         return Problem(name, (0.0, 1.0, 0.0, 1.0), g, capi.BC_FIXED, 0.15, 0.6, rotor_pri,
                        {"amp": amp}, bc_state=st)
+    if name == "cloud_shock":  # main.f90:141-155
+        g = 5.0 / 3.0 if gamma is None else gamma
+        st = pri2con(np.array([1.0, -11.2536, 0.0, 0.0, 0.0, 0.56418958, 0.56418958, 1.0]), g)
+        return Problem(name, (0.0, 1.0, 0.0, 1.0), g, capi.BC_CLOUD_SHOCK, 0.06, 0.6, cloud_shock_pri, {},
+                       bc_state=st)
+    if name == "jet":  # main.f90:156-169; nx must be a multiple of 10 (the nozzle is the first nx/10)
+        g = 1.4 if gamma is None else gamma
+        st = pri2con(np.array([g, 0.0, 800.0, 0.0, 0.0, math.sqrt(200.0), 0.0, 1.0]), g)
+        return Problem(name, (0.0, 0.5, 0.0, 1.5), g, capi.BC_JET, 2.0e-3, 0.6, jet_pri, {}, bc_state=st)
     if name == "alfven":
         g = 5.0 / 3.0 if gamma is None else gamma
         return Problem(name, (0.0, 1.0 / math.cos(PI / 6.0), 0.0, 1.0 / math.sin(PI / 6.0)), g,

@@ -85,6 +85,6 @@ def test_set_up_entry_points_reject_bad_arguments(pkg):
 
 
 def test_every_problem_has_a_device_initial_state(pkg):
-    for name in ("ot2pi", "ot_unit", "vortex", "blast", "rotor", "alfven"):
+    for name in ("ot2pi", "ot_unit", "vortex", "blast", "rotor", "alfven", "cloud_shock", "jet"):
         pid, params = pkg.problems.make(name).device_ic()
-        assert 0 <= pid <= 5 and len(params) in (1, 2, 5)
+        assert 0 <= pid <= 7 and len(params) in (1, 2, 5)

@@ -16,7 +16,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SETUPS = [("ot2pi", {}), ("ot_unit", {"amp": 0.8}), ("vortex", {}), ("blast", {}), ("rotor", {"amp": 1.3}),
-          ("alfven", {})]
+          ("alfven", {}), ("cloud_shock", {}), ("jet", {})]
 
 
 def _make(pkg, name, kw):
