@@ -23,7 +23,11 @@ template <int P>
 struct ResCfg;
 // MHD_RES_CFG<p> = TX, TY, NT, MINB, HW, where HW = warps that start phase 2 on the interface
 // fluxes (all warps then share the node pairs through a shared-memory work counter).  The values
-// below were chosen by timing on B200; a build may override them (-DMHD_RES_CFG3=...).
+// below were chosen by timing on B200.  autotune.py (next to build.py) times candidate sets on the
+// GPU at hand and writes residual_tuned.h, which takes precedence when present.
+#if __has_include("residual_tuned.h")
+#include "residual_tuned.h"
+#endif
 #ifndef MHD_RES_CFG1
 #define MHD_RES_CFG1 8, 4, 128, 4, 3
 #endif
@@ -83,6 +87,8 @@ struct ResLayout {
   static constexpr int O_RED = O_PT + TE * NN;
   static constexpr int TOTAL = O_RED + 32;  // O_RED + 16 doubles also hold the pair work counter
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
+  static_assert(BYTES <= 227 * 1024, "residual tile does not fit the shared memory of one CTA");
+  static_assert(ResCfg<P>::NT % 32 == 0 && ResCfg<P>::NT <= 512, "whole warps, at most 16");
 };
 
 // pair index within a line -> (a, b), b < a, enumerated a = 1..N-1, b = 0..a-1
