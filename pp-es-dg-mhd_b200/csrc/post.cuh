@@ -56,6 +56,46 @@ __device__ __forceinline__ double grp_max(double v) {
   return v;
 }
 
+// All eight sums of a[0..7] over each group of GS lanes, in every lane of the group, by a
+// reduce-scatter (each exchange halves the values a lane carries, one lane bit per level) and an
+// all-gather: 8 + 7 exchanges at GS = 16 instead of 8 butterflies of 4.  Deterministic, and every
+// lane of a group ends with the same sums (each final sum is formed in one lane pair as x + y and
+// y + x, which IEEE addition makes equal, and gathered from one lane).
+template <int GS>
+__device__ __forceinline__ void grp_sum8(double* a) {
+  constexpr int LV = GS >= 8 ? 3 : (GS == 4 ? 2 : 1);  // halving levels
+  const int lane = threadIdx.x & 31;
+  constexpr int CNT = 8 >> LV;                          // values a lane keeps after them
+#pragma unroll
+  for (int j = 0; j < LV; ++j) {
+    const int o = GS >> (j + 1);
+    const int half = 4 >> j;
+    const bool hi = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < half; ++i) {
+      const double send = hi ? a[i] : a[i + half];
+      const double recv = __shfl_xor_sync(FULL_MASK, send, o);
+      a[i] = (hi ? a[i + half] : a[i]) + recv;
+    }
+  }
+#pragma unroll
+  for (int o = GS >> (LV + 1); o > 0; o >>= 1)
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) a[i] = a[i] + __shfl_xor_sync(FULL_MASK, a[i], o);
+  const int gbase = lane & ~(GS - 1);
+  double out[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    int src = gbase;
+#pragma unroll
+    for (int j = 0; j < LV; ++j)
+      if (v & (4 >> j)) src += GS >> (j + 1);
+    out[v] = __shfl_sync(FULL_MASK, a[v & (CNT - 1)], src);
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) a[v] = out[v];
+}
+
 __device__ __forceinline__ double node_prs(const double* x, double gamma) {
   return prs_of(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], gamma);
 }
@@ -150,12 +190,12 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
                                                  int ent_offset, double* __restrict__ partial_out,  // 8 doubles
                                                  double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                                                  unsigned char* __restrict__ cell_ent_nan, int limit,
-                                                 const double* s_A, double* s_red, int* s_cnt, double* run_max,
-                                                 double* run_min) {
+                                                 const double* s_A, double* s_ldf, double* s_red, int* s_cnt,
+                                                 double* run_max, double* run_min) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grp = lane / GS, node = lane - grp * GS, gbase = grp * GS;
+  const int grp = lane / GS, node = lane - grp * GS;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long total = (long long)NXG * (ny + 2);
   const long long e0 = chunk * TE;
@@ -181,7 +221,8 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   const double w = nd ? 0.25 * dc.qw[k] * dc.qw[l] : 0.0;
   double avg[8];
 #pragma unroll
-  for (int v = 0; v < 8; ++v) avg[v] = grp_sum<GS>(w * x[v]);
+  for (int v = 0; v < 8; ++v) avg[v] = w * x[v];
+  grp_sum8<GS>(avg);
   // admissibility of the average (DG_solver.f90:186-193): an inadmissible element is left unwritten
   if (valid) {
     const double prs = prs_of(avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6], avg[7], gamma);
@@ -205,19 +246,22 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   }
   // LDF projection of (Bx - avg, By - avg) with the dense nodal operator: this lane forms the
   // outputs at its node (rows `node` and NN + node); the inputs come from the group's lanes
-  if (apply_ldf) {
-    double ox = 0.0, oy = 0.0;
-#pragma unroll 4
-    for (int m = 0; m < NN; ++m) {
-      const double bxm = __shfl_sync(FULL_MASK, x[4], gbase + m) - avg[4];
-      const double bym = __shfl_sync(FULL_MASK, x[5], gbase + m) - avg[5];
-      if (nd) {
-        ox += s_A[node + N2 * m] * bxm;
-        oy += s_A[NN + node + N2 * m] * bxm;
-        ox += s_A[node + N2 * (NN + m)] * bym;
-        oy += s_A[NN + node + N2 * (NN + m)] * bym;
-      }
+  if (apply_ldf) {  // the group's (Bx, By) - avg pass through a padded per-group shared row
+    double* sb = s_ldf + (warp * G + grp) * (N2 + 1);
+    if (nd) {
+      sb[node] = x[4] - avg[4];
+      sb[NN + node] = x[5] - avg[5];
     }
+    __syncwarp();
+    double ox = 0.0, oy = 0.0;
+    if (nd)
+#pragma unroll 8
+      for (int m = 0; m < N2; ++m) {
+        const double b = sb[m];
+        ox += s_A[node + N2 * m] * b;
+        oy += s_A[NN + node + N2 * m] * b;
+      }
+    __syncwarp();  // the row is rewritten by the next chunk
     if (valid) {
       x[4] = ox + avg[4];
       x[5] = oy + avg[5];
@@ -313,6 +357,7 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
                       unsigned char* __restrict__ cell_ent_nan, int limit, int nchunks) {
   using C = PPCfg<P>;
   __shared__ double s_A[C::N2 * C::N2];
+  __shared__ double s_ldf[C::TE * (C::N2 + 1)];
   __shared__ double s_red[C::TE * 8 + 128];
   __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
@@ -328,7 +373,7 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
   for (int c = blockIdx.x; c < nchunks; c += gridDim.x)
     pp_avg_ldf_chunk<P, NEEDG>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
                                partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit, s_A,
-                               s_red, &s_cnt, run_max, run_min);
+                               s_ldf, s_red, &s_cnt, run_max, run_min);
   __syncthreads();
   if (NEEDG && need_global) flush_minmax(run_max, run_min, s_red, ctrl);
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
@@ -343,6 +388,7 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate) {
   using C = PPCfg<P>;
   __shared__ double s_A[C::N2 * C::N2];
+  __shared__ double s_ldf[C::TE * (C::N2 + 1)];
   __shared__ double s_red[C::TE * 8 + 128];
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
@@ -367,7 +413,7 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     const int need_global = FINAL && d.use_oedg;
     pp_avg_ldf_chunk<P, FINAL>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global, d.ent_offset,
                                d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan, !FINAL,
-                               s_A, s_red, &s_cnt, run_max, run_min);
+                               s_A, s_ldf, s_red, &s_cnt, run_max, run_min);
     __syncthreads();
     if (need_global) flush_minmax(run_max, run_min, s_red, d.ctrl);  // per item: members differ
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
