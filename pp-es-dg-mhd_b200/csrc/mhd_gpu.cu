@@ -199,10 +199,10 @@ void launch_bc(mhd_gpu* h, double* u, int gate) {
 }
 
 template <int P>
-void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate) {
+void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate, StageCombine sc = StageCombine{}) {
   using L = ResLayout<P>;
   dim3 grid((h->nx + L::TX - 1) / L::TX, (h->ny + L::TY - 1) / L::TY);
-  residual_kernel<P><<<grid, ResCfg<P>::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate);
+  residual_kernel<P><<<grid, ResCfg<P>::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate, sc);
 }
 
 template <int P>
@@ -280,22 +280,36 @@ void fill_status(const mhd_gpu* h, mhd_gpu_status* st) {
 }
 
 // one try of a time step (drive.f90:93-300), recorded into the capturing stream
+// the combination of stage `stage` (SSP-RK(2,2) stage 2, SSP-RK(3,3) stages 2 and 3; the
+// coefficients of combine_value) folded into the previous residual; none otherwise
+StageCombine next_stage_combine(const mhd_gpu* h, int stage) {
+  StageCombine sc{};
+  if (h->R == 2 && stage == 2) {
+    sc = StageCombine{h->u[0], h->u[2], 0.5, 0.5, &h->ctrl->dt};
+  } else if (h->R == 3 && (stage == 2 || stage == 3)) {
+    sc = StageCombine{h->u[0], h->u[stage], stage == 2 ? 0.75 : 1.0 / 3.0, stage == 2 ? 0.25 : 2.0 / 3.0, &h->ctrl->dt};
+  }
+  return sc;
+}
+
 template <int P>
 void enqueue_try(mhd_gpu* h) {
   const int R = h->R;
   ctl_step_begin<<<1, 1, 0, h->stream>>>(h->ctrl);
   launch_residual<P>(h, h->u[0], h->ut[1], ST_RECOMPUTE);
   ctl_dt<<<1, 1, 0, h->stream>>>(h->ctrl);
+  // SSP-RK(2,2) and (3,3): stages after the first take their combination from the previous
+  // stage's residual (next_stage_combine); SSP-RK(1,1) and (5,4) keep the separate combine
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
     ctl_stage_time<<<1, 1, 0, h->stream>>>(h->ctrl, R, s);
-    launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
+    if (s == 1 || R > 3) launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
     launch_bc<P>(h, h->u[s], ST_RUN);
     launch_post<P>(h, s, h->use_oedg && fin, h->use_ldf, &h->ctrl->dt, 0.0, h->ent_offset, fin,
                    fin ? h->u[0] : nullptr, ST_RUN, 1);
     ctl_stage_end<<<1, 1, 0, h->stream>>>(h->ctrl);
     launch_bc<P>(h, h->u[s], ST_RUN);
-    launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN);
+    launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN, fin ? StageCombine{} : next_stage_combine(h, s + 1));
   }
   ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R);
 }
@@ -868,17 +882,17 @@ extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, 
   switch (p) {
     case 1: {
       using L = ResLayout<1>;
-      residual_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<1>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS);
+      residual_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<1>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     case 2: {
       using L = ResLayout<2>;
-      residual_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<2>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS);
+      residual_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<2>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     default: {
       using L = ResLayout<3>;
-      residual_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<3>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS);
+      residual_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<3>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
   }

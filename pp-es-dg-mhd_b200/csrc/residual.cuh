@@ -105,12 +105,23 @@ __device__ __forceinline__ int pair_index(int a, int b) { return a * (a - 1) / 2
 // swap_xy (DG_solver.f90:1556-1568) as a variable permutation: 1 <-> 2, 4 <-> 5
 __host__ __device__ constexpr int swap_xy_var(int v) { return v == 1 ? 2 : v == 2 ? 1 : v == 4 ? 5 : v == 5 ? 4 : v; }
 
+// The next stage's SSP-RK combination folded into the residual (drive.f90:185-241 for SSP-RK3,
+// :148-183 for SSP-RK(2,2)): out = ca*u0 + cb*(u + dt*L(u)), rounded exactly as combine_value
+// forms it, written to the interior of the next stage's state instead of storing L(u).  Only
+// where that combination uses no other stage's L (u0 == nullptr: plain residual into ut).
+struct StageCombine {
+  const double* u0;     // u_con (ghosted layout)
+  double* out;          // the next stage's state (ghosted layout)
+  double ca, cb;
+  const double* dt;     // the try's dt (device control block)
+};
+
 // One tile of the residual: elements (tile_x*TX + 1 .. , tile_y*TY + 1 .. ) of the instance
 // described by (u, ut, g, ctrl).  All threads of the CTA call it with the same arguments.
 template <int P>
 __device__ __forceinline__ void residual_tile(const double* __restrict__ u, double* __restrict__ ut,
                                               const Geo& g, Ctrl* ctrl, int tile_x, int tile_y,
-                                              double* sm) {
+                                              double* sm, const StageCombine& sc = StageCombine{}) {
   using L = ResLayout<P>;
   constexpr int N = L::N, NN = L::NN, EB = L::EB, ES = L::ES, TX = L::TX, TY = L::TY, TE = L::TE;
   constexpr int NT = ResCfg<P>::NT;
@@ -374,6 +385,13 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
       }
+      if (sc.u0) {  // the next stage's state instead of L(u)
+        const double* u0n = sc.u0 + (((long long)(j0 + er) * (nx + 2)) + (i0 + ec)) * EB + q;
+        const double dt = *sc.dt;
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+          acc[v] = __dadd_rn(__dmul_rn(sc.ca, u0n[v * NN]), __dmul_rn(sc.cb, __dadd_rn(w[v], __dmul_rn(dt, acc[v]))));
+      }
 #pragma unroll
       for (int v = 0; v < 8; ++v) cw[v * NN] = acc[v];  // own node only: safe in place
     } else {
@@ -416,7 +434,8 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
     for (int it = tid; it < H * V2; it += NT) {
       const int r = it / V2, c = it - r * V2;
       if (c < W * EB / 2) {
-        double2* dst = reinterpret_cast<double2*>(ut + ((long long)(j0 + r - 1) * nx + (i0 - 1)) * EB);
+        double2* dst = sc.u0 ? reinterpret_cast<double2*>(sc.out + ((long long)(j0 + r) * (nx + 2) + i0) * EB)
+                             : reinterpret_cast<double2*>(ut + ((long long)(j0 + r - 1) * nx + (i0 - 1)) * EB);
         const int ec = (ES == EB) ? 0 : c / (EB / 2), cw = c - ec * (EB / 2);
         dst[c] = reinterpret_cast<const double2*>(s_cons + (r * TX + ec) * ES)[cw];
       }
@@ -427,10 +446,11 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
 // single instance: one CTA per tile
 template <int P>
 __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
-    residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate) {
+    residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
+                    StageCombine sc) {
   if (!gate_open(ctrl, gate)) return;
   extern __shared__ __align__(16) double sm[];
-  residual_tile<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm);
+  residual_tile<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, sc);
 }
 
 // many instances of degree P: a persistent grid walks every member's tiles (row-major per member);
