@@ -217,12 +217,14 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
   const int grid_res = gr.res, grid_cmb = gr.cmb, grid_bc = gr.bc, grid_avg = gr.avg, grid_sig = gr.sig,
             grid_lim = gr.lim;
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_BEGIN, R, 0);
-  residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE);
+  residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE,
+                                                              0, 0.0, 0.0);
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_DT, R, 0);
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_TIME, R, s);
-    combine_batched<EB><<<grid_cmb, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
+    if (s == 1 || R > 3)  // SSP-RK(2,2)/(3,3): later stages come from the previous residual
+      combine_batched<EB><<<grid_cmb, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
     bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
     if (fin)
       pp_avg_ldf_batched<P, true><<<gr.avg_final, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN);
@@ -236,7 +238,12 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
     if (fin) pp_entsum_batched<<<b->nsm, 256, 0, st>>>(in, ninst, ST_RUN);
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_END, R, s);
     bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
-    residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, s, (s % R) + 1, ST_RUN);
+    // the coefficients of combine_value for SSP-RK(2,2) stage 2 and SSP-RK(3,3) stages 2, 3
+    const int nxt = (!fin && (R == 2 || R == 3)) ? s + 1 : 0;
+    const double ca = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.75 : 1.0 / 3.0));
+    const double cb = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.25 : 2.0 / 3.0));
+    residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, s, (s % R) + 1,
+                                                                ST_RUN, nxt, ca, cb);
   }
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_END, R, 0);
 }

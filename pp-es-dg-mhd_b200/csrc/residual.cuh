@@ -454,11 +454,13 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
 }
 
 // many instances of degree P: a persistent grid walks every member's tiles (row-major per member);
-// the state is slot `src`, the result goes to ut[dst]
+// the state is slot `src`, the result goes to ut[dst], or (next_stage > 0) the combination of
+// stage next_stage goes to slot next_stage
 template <int P>
 __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
     residual_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
-                     const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate) {
+                     const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate,
+                     int next_stage, double ca, double cb) {
   extern __shared__ __align__(16) double sm[];
   const int nw = *nwork, n = *ninst;
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
@@ -466,7 +468,9 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
     const int ntx = (d.g.nx + ResCfg<P>::TX - 1) / ResCfg<P>::TX;
-    residual_tile<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm);
+    // next_stage > 0: that stage's combination is folded in (the group's rknstg is uniform)
+    const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
+    residual_tile<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, sc);
     __syncthreads();  // the next tile reuses shared memory
   }
 }
