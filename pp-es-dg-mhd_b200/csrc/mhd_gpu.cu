@@ -31,6 +31,8 @@ struct mhd_gpu {
   int device;
   cudaStream_t stream;
   cudaStream_t own_stream;
+  cudaStream_t side_stream;  // the OEDG global sums run here beside the face indicators
+  cudaEvent_t ev_fork, ev_join;
   double* u[6];   // slot 0 = u_con, s = uRK_con(:,s)
   double* ut[6];  // 1..R
   double* u_avg;
@@ -235,10 +237,14 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
                                                                  h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
   }
   if (limit_in_loop1) return;
-  if (apply_oedg) {
-    pp_reduce_kernel<<<1, 256, 0, h->stream>>>(h->partial, nb1, h->ctrl, gate);
+  if (apply_oedg) {  // the global sums (one CTA) and the face indicators are independent: fork/join
+    cudaEventRecord(h->ev_fork, h->stream);
+    cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0);
+    pp_reduce_kernel<<<1, 256, 0, h->side_stream>>>(h->partial, nb1, h->ctrl, gate);
+    cudaEventRecord(h->ev_join, h->side_stream);
     const dim3 gs((h->nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX, (h->ny + SigCfg<P>::TY - 1) / SigCfg<P>::TY);
     pp_sigsum_kernel<P><<<gs, 256, 0, h->stream>>>(h->u[slot], h->geo, h->ctrl, gate, h->sig_x, h->sig_y);
+    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
   }
   dim3 g3 = pp_grid_limit<P>(h);
   pp_limit_kernel<P><<<g3, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_oedg, dt_ptr,
@@ -333,6 +339,12 @@ int build_step_graph(mhd_gpu* h) {
 void free_all(mhd_gpu* h) {
   if (!h) return;
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  if (h->side_stream) {
+    cudaStreamSynchronize(h->side_stream);
+    cudaStreamDestroy(h->side_stream);
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaStream_t fs = h->own_stream;  // a stream-ordered free back into the device pool
   if (h->block && h->owns_block) cudaFreeAsync(h->block, fs);
   if (fs) {
@@ -420,7 +432,11 @@ int create_instance(int nx, int ny, int px, int py, int rknstg, double left, dou
   h->hy = (top - bottom) / ny;
   for (int v = 0; v < 8; ++v) h->bc_state[v] = bc_state8 ? bc_state8[v] : 0.0;
   cudaMemPool_t pool;
-  if (device_pool(h->device, &pool) || cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (device_pool(h->device, &pool) || cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    free_all(h);
     delete h;
     return MHD_ERR_CUDA;
   }
