@@ -118,13 +118,18 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
   constexpr double BIG = 1.7976931348623157e308;
   const double gamma = g.gamma;
   const DegConst& dc = c_deg[P];
-  // density: theta from the minimum nodal density (DG_solver.f90:538-553)
-  const double den_min = grp_min<GS>(active ? x[0] : BIG);
+  // density: theta from the minimum nodal density (DG_solver.f90:538-553).  The minimum only
+  // matters below PP_EPS, so the reduction runs only when some lane of the warp is below it.
   double thd = -1.0;
-  if (den_min < PP_EPS) thd = fmax(fmin((avg[0] - PP_EPS) / (avg[0] - den_min), 1.0), 0.0);
+  if (__any_sync(FULL_MASK, active && x[0] < PP_EPS)) {
+    const double den_min = grp_min<GS>(active ? x[0] : BIG);
+    if (den_min < PP_EPS) thd = fmax(fmin((avg[0] - PP_EPS) / (avg[0] - den_min), 1.0), 0.0);
+  }
   if (active && thd >= 0.0) x[0] = fmax(avg[0] + thd * (x[0] - avg[0]), PP_EPS);
-  // pressure: theta from the minimum nodal pressure (DG_solver.f90:556-571)
-  const double pmin = grp_min<GS>(active ? node_prs(x, gamma) : BIG);
+  // pressure: theta from the minimum nodal pressure (DG_solver.f90:556-571), likewise
+  const double pq = active ? node_prs(x, gamma) : BIG;
+  double pmin = BIG;
+  if (__any_sync(FULL_MASK, pq < PP_EPS)) pmin = grp_min<GS>(pq);
   double thp = -1.0;
   if (pmin < PP_EPS) {
     const double pa = prs_of(avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6], avg[7], gamma);
