@@ -88,3 +88,28 @@ def test_every_problem_has_a_device_initial_state(pkg):
     for name in ("ot2pi", "ot_unit", "vortex", "blast", "rotor", "alfven", "cloud_shock", "jet"):
         pid, params = pkg.problems.make(name).device_ic()
         assert 0 <= pid <= 7 and len(params) in (1, 2, 5)
+
+
+def test_autotune_candidates_are_well_formed():
+    """every candidate set of the residual autotuner gives each degree whole warps within one CTA"""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("autotune", os.path.join(ROOT, "pp-es-dg-mhd_b200", "autotune.py"))
+    at = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(at)
+    sets = {len(c) for c in at.CANDIDATES.values()}
+    assert len(sets) == 1  # set i takes candidate i of every degree
+    for p, cands in at.CANDIDATES.items():
+        for tx, ty, nt, minb, hw in cands:
+            assert nt % 32 == 0 and nt <= 512 and 1 <= hw <= nt // 32 and tx >= 1 and ty >= 1 and minb >= 1
+
+
+def test_tuned_header_defines_every_degree():
+    path = os.path.join(ROOT, "pp-es-dg-mhd_b200", "csrc", "residual_tuned.h")
+    if not os.path.exists(path):
+        return
+    text = open(path).read()
+    for p in (1, 2, 3):
+        m = re.search(rf"#define MHD_RES_CFG{p} (\d+), (\d+), (\d+), (\d+), (\d+)", text)
+        assert m, p
+        tx, ty, nt, minb, hw = map(int, m.groups())
+        assert nt % 32 == 0 and 1 <= hw <= nt // 32
