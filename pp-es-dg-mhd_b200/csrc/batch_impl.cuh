@@ -223,13 +223,17 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
     ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_TIME, R, s);
-    if (s == 1 || R > 3)  // SSP-RK(2,2)/(3,3): later stages come from the previous residual
+    // stage 1: loop 1 forms the stage state and its ghost ring; SSP-RK(2,2)/(3,3): later stages
+    // come from the previous residual
+    if (s > 1 && R > 3)
       combine_batched<EB><<<grid_cmb, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
-    bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
+    if (s > 1) bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
     if (fin)
-      pp_avg_ldf_batched<P, true><<<gr.avg_final, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN);
+      pp_avg_ldf_batched<P, true><<<gr.avg_final, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN,
+                                                                  s == 1);
     else
-      pp_avg_ldf_batched<P, false><<<grid_avg, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN);
+      pp_avg_ldf_batched<P, false><<<grid_avg, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN,
+                                                                s == 1);
     if (fin) {
       pp_reduce_batched<<<b->nsm, 256, 0, st>>>(in, ninst, fin, ST_RUN);
       pp_sigsum_batched<P><<<grid_sig, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);

@@ -221,20 +221,23 @@ void launch_combine(mhd_gpu* h, int stage, const double* dt_ptr, double dt, int 
 template <int P>
 // fuse = 1 (time-step pipeline only): a stage without OEDG, entropy or acceptance copy runs loops
 // 1 and 3 in one kernel (the stage result is discarded if an average is inadmissible)
+// s1 (time-step pipeline, stage 1 only): loop 1 forms the stage state from u0 and the stage-1
+// residual, with its ghost ring, in place of the combination and boundary-fill launches
 void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const double* dt_ptr, double oedg_dt,
-                 int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0) {
+                 int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0,
+                 Stage1Src s1 = Stage1Src{}) {
   const int nb1 = pp_nblk_avg<P>(h);
   const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
   if (apply_oedg) {
     const int grid1 = std::min(nb1, pp_resident_ctas<P, true>(h->device));
     pp_avg_ldf_kernel<P, true><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
                                                                 1, ent_offset, h->partial, h->cell_ent_DG,
-                                                                h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
+                                                                h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1, s1);
   } else {
     const int grid1 = std::min(nb1, pp_resident_ctas<P, false>(h->device));
     pp_avg_ldf_kernel<P, false><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
                                                                  0, ent_offset, h->partial, h->cell_ent_DG,
-                                                                 h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1);
+                                                                 h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1, s1);
   }
   if (limit_in_loop1) return;
   if (apply_oedg) {  // the global sums (one CTA) and the face indicators are independent: fork/join
@@ -309,10 +312,12 @@ void enqueue_try(mhd_gpu* h) {
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
     ctl_stage_time<<<1, 1, 0, h->stream>>>(h->ctrl, R, s);
-    if (s == 1 || R > 3) launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
-    launch_bc<P>(h, h->u[s], ST_RUN);
+    // stage 1: loop 1 forms the stage state and its ghost ring (Stage1Src)
+    if (s > 1 && R > 3) launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
+    if (s > 1) launch_bc<P>(h, h->u[s], ST_RUN);
+    const Stage1Src s1 = s == 1 ? Stage1Src{h->u[0], h->ut[1], &h->ctrl->dt, stage1_coef(R)} : Stage1Src{};
     launch_post<P>(h, s, h->use_oedg && fin, h->use_ldf, &h->ctrl->dt, 0.0, h->ent_offset, fin,
-                   fin ? h->u[0] : nullptr, ST_RUN, 1);
+                   fin ? h->u[0] : nullptr, ST_RUN, 1, s1);
     ctl_stage_end<<<1, 1, 0, h->stream>>>(h->ctrl);
     launch_bc<P>(h, h->u[s], ST_RUN);
     launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN, fin ? StageCombine{} : next_stage_combine(h, s + 1));

@@ -9,7 +9,54 @@ enum BcKind : int {
   BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_FIXED = 2, BC_XEXTRAP_YPER = 3, BC_CLOUD_SHOCK = 4, BC_JET = 5
 };
 
-// Ghost-ring fill (problems.f90:312-423,597-654).  One thread per ghost value; corners untouched.
+// Where a ghost value comes from (problems.f90:312-423,597-654): node sq of variable v of interior
+// element (si, sj), negated if neg, or the fixed state bc_state[v] if fixed.  (i, j) is a ghost
+// element off the corners, q its node.
+struct BcSrc {
+  int si, sj, sq;
+  bool fixed, neg;
+};
+
+template <int P>
+__device__ __forceinline__ BcSrc bc_source(const Geo& g, int i, int j, int v, int q) {
+  constexpr int N = P + 1;
+  const int nx = g.nx, ny = g.ny, k = q % N, l = q / N;
+  const bool xside = (i == 0 || i == nx + 1);  // left/right ghost column
+  BcSrc s{i, j, q, false, false};
+  int kind = g.bc_kind;
+  if (kind == BC_CLOUD_SHOCK || kind == BC_JET) {
+    // BC_cloud_shock (problems.f90:449-471): element copies, inflow state on the right.
+    // BC_jet1_cell_ext (problems.f90:502-593): mirror of element 1 on the left (k <- n-1-k, normal
+    // momentum and field negated), copies elsewhere, the nozzle state below i <= nx/10.
+    if ((kind == BC_CLOUD_SHOCK && i == nx + 1) || (kind == BC_JET && j == 0 && i <= nx / 10)) {
+      s.fixed = true;
+      return s;
+    }
+    s.si = (i == 0) ? 1 : (i == nx + 1 ? nx : i);
+    s.sj = (j == 0) ? 1 : (j == ny + 1 ? ny : j);
+    if (kind == BC_JET && i == 0) {
+      s.sq = (N - 1 - k) + N * l;
+      s.neg = (v == 1 || v == 4);
+    }
+    return s;
+  }
+  if (kind == BC_XEXTRAP_YPER) kind = xside ? BC_EXTRAPOLATE : BC_PERIODIC;
+  if (kind == BC_FIXED) {
+    s.fixed = true;
+  } else if (kind == BC_PERIODIC) {
+    s.si = (i == 0) ? nx : (i == nx + 1 ? 1 : i);
+    s.sj = (j == 0) ? ny : (j == ny + 1 ? 1 : j);
+  } else if (xside) {  // extrapolation of the adjacent interior trace
+    s.si = (i == 0) ? 1 : nx;
+    s.sq = ((i == 0) ? 0 : N - 1) + N * l;
+  } else {
+    s.sj = (j == 0) ? 1 : ny;
+    s.sq = k + N * ((j == 0) ? 0 : N - 1);
+  }
+  return s;
+}
+
+// Ghost-ring fill.  One thread per ghost value; corners untouched.
 template <int P>
 __device__ __forceinline__ void bc_value(double* __restrict__ u, const Geo& g, long long it) {
   constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
@@ -17,61 +64,20 @@ __device__ __forceinline__ void bc_value(double* __restrict__ u, const Geo& g, l
   const long long nghost = 2LL * (nx + ny);
   if (it >= nghost * EB) return;
   const int ge = (int)(it / EB), vi = (int)(it - (long long)ge * EB);
-  const int v = vi / NN, q = vi - v * NN, k = q % N, l = q / N;
-  int i, j;        // ghost element
-  int si, sj, sq;  // source element and node
-  bool xside;      // left/right ghost column
-  if (ge < ny) { i = 0; j = 1 + ge; xside = true; }
-  else if (ge < 2 * ny) { i = nx + 1; j = 1 + ge - ny; xside = true; }
-  else if (ge < 2 * ny + nx) { i = 1 + ge - 2 * ny; j = 0; xside = false; }
-  else { i = 1 + ge - 2 * ny - nx; j = ny + 1; xside = false; }
+  const int v = vi / NN, q = vi - v * NN;
+  int i, j;  // ghost element
+  if (ge < ny) { i = 0; j = 1 + ge; }
+  else if (ge < 2 * ny) { i = nx + 1; j = 1 + ge - ny; }
+  else if (ge < 2 * ny + nx) { i = 1 + ge - 2 * ny; j = 0; }
+  else { i = 1 + ge - 2 * ny - nx; j = ny + 1; }
   const long long dst = ((long long)j * NXG + i) * EB + vi;
-  int kind = g.bc_kind;
-  if (kind == BC_CLOUD_SHOCK || kind == BC_JET) {
-    // BC_cloud_shock (problems.f90:449-471): element copies, inflow state on the right.
-    // BC_jet1_cell_ext (problems.f90:502-593): mirror of element 1 on the left (k <- n-1-k, normal
-    // momentum and field negated), copies elsewhere, the nozzle state below i <= nx/10.
-    double sign = 1.0;
-    if (kind == BC_CLOUD_SHOCK && i == nx + 1) {
-      u[dst] = g.bc_state[v];
-      return;
-    }
-    if (kind == BC_JET && j == 0 && i <= nx / 10) {
-      u[dst] = g.bc_state[v];
-      return;
-    }
-    si = (i == 0) ? 1 : (i == nx + 1 ? nx : i);
-    sj = (j == 0) ? 1 : (j == ny + 1 ? ny : j);
-    sq = q;
-    if (kind == BC_JET && i == 0) {
-      sq = (N - 1 - k) + N * l;
-      if (v == 1 || v == 4) sign = -1.0;
-    }
-    const double x = u[((long long)sj * NXG + si) * EB + v * NN + sq];
-    u[dst] = sign < 0.0 ? -x : x;
-    return;
-  }
-  if (kind == BC_XEXTRAP_YPER) kind = xside ? BC_EXTRAPOLATE : BC_PERIODIC;
-  if (kind == BC_FIXED) {
+  const BcSrc s = bc_source<P>(g, i, j, v, q);
+  if (s.fixed) {
     u[dst] = g.bc_state[v];
     return;
   }
-  if (kind == BC_PERIODIC) {
-    si = (i == 0) ? nx : (i == nx + 1 ? 1 : i);
-    sj = (j == 0) ? ny : (j == ny + 1 ? 1 : j);
-    sq = q;
-  } else {  // extrapolation of the adjacent interior trace
-    if (xside) {
-      si = (i == 0) ? 1 : nx;
-      sj = j;
-      sq = ((i == 0) ? 0 : N - 1) + N * l;
-    } else {
-      si = i;
-      sj = (j == 0) ? 1 : ny;
-      sq = k + N * ((j == 0) ? 0 : N - 1);
-    }
-  }
-  u[dst] = u[((long long)sj * NXG + si) * EB + v * NN + sq];
+  const double x = u[((long long)s.sj * NXG + s.si) * EB + v * NN + s.sq];
+  u[dst] = s.neg ? -x : x;
 }
 
 template <int P>
@@ -99,6 +105,9 @@ __global__ void __launch_bounds__(256) bc_batched(const InstDesc* __restrict__ i
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 
+// the weight of dt in the stage-1 update u0 + (weight*dt)*k1
+__host__ __device__ constexpr double stage1_coef(int R) { return R == 5 ? 0.391752226571890 : 1.0; }
+
 template <int EB>
 __device__ __forceinline__ void combine_value(
     const double* __restrict__ u0, const double* __restrict__ r1, const double* __restrict__ r2,
@@ -125,7 +134,7 @@ __device__ __forceinline__ void combine_value(
       val = add(mul(1.0 / 3.0, u0[gi]), mul(2.0 / 3.0, add(r2[gi], mul(dt, k3[ki]))));
   } else {  // SSP-RK(5,4)
     switch (stage) {
-      case 1: val = add(u0[gi], mul(mul(0.391752226571890, dt), k1[ki])); break;
+      case 1: val = add(u0[gi], mul(mul(stage1_coef(5), dt), k1[ki])); break;
       case 2: val = add(add(mul(0.444370493651235, u0[gi]), mul(0.555629506348765, r1[gi])), mul(mul(0.368410593050371, dt), k2[ki])); break;
       case 3: val = add(add(mul(0.620101851488403, u0[gi]), mul(0.379898148511597, r2[gi])), mul(mul(0.251891774271694, dt), k3[ki])); break;
       case 4: val = add(add(mul(0.178079954393132, u0[gi]), mul(0.821920045606868, r3[gi])), mul(mul(0.544974750228521, dt), k4[ki])); break;

@@ -22,6 +22,7 @@
 // elements; per-chunk partial sums are formed in element order.
 #pragma once
 #include "common.cuh"
+#include "misc.cuh"
 
 namespace mhd {
 
@@ -189,6 +190,37 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
 // on neg_avg (the time-step pipeline re-tries the step from u_con), so the stand-alone
 // post_process never fuses.
 // ---------------------------------------------------------------------------------------------
+// Stage-1 source of loop 1 (time-step pipeline only).  With u0 set, the stage state is formed
+// here instead of being read from u: u0 + (coef*dt)*k1 on interior elements, rounded as
+// combine_value rounds stage 1, and the ghost ring from those values by bc_source, as the boundary
+// fill would leave it.  Every element is then written back, the inadmissible ones unchanged.
+struct Stage1Src {
+  const double* u0;  // state at the start of the step (ghosted layout)
+  const double* k1;  // stage-1 residual (interior layout)
+  const double* dt;
+  double coef;       // 1 for SSP-RK(1,1), (2,2), (3,3); the first stage weight of SSP-RK(5,4)
+};
+
+template <int P>
+__device__ __forceinline__ double stage1_node(const Stage1Src& s1, const Geo& g, int i, int j, bool inner, int v,
+                                              int q, double dts) {
+  constexpr int NN = (P + 1) * (P + 1), EB = 8 * NN;
+  int si = i, sj = j, sq = q;
+  bool neg = false;
+  if (!inner) {
+    const BcSrc b = bc_source<P>(g, i, j, v, q);
+    if (b.fixed) return g.bc_state[v];
+    si = b.si;
+    sj = b.sj;
+    sq = b.sq;
+    neg = b.neg;
+  }
+  const long long gi = ((long long)sj * (g.nx + 2) + si) * EB + v * NN + sq;
+  const long long ki = ((long long)(sj - 1) * g.nx + (si - 1)) * EB + v * NN + sq;
+  const double x = __dadd_rn(s1.u0[gi], __dmul_rn(dts, s1.k1[ki]));
+  return neg ? -x : x;
+}
+
 template <int P, bool NEEDG>
 __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg, const Geo& g,
                                                  Ctrl* ctrl, long long chunk, int apply_ldf, int need_global,
@@ -196,7 +228,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
                                                  double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                                                  unsigned char* __restrict__ cell_ent_nan, int limit,
                                                  const double* s_A, double* s_ldf, double* s_red, int* s_cnt,
-                                                 double* run_max, double* run_min) {
+                                                 double* run_max, double* run_min, const Stage1Src& s1) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -210,8 +242,10 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   const DegConst& dc = c_deg[P];
   const double gamma = g.gamma;
   bool valid = false, inner = false;
+  int i = 0, j = 0;
   if (el < ne) {
-    const int j = (int)(e / NXG), i = (int)(e - (long long)j * NXG);
+    j = (int)(e / NXG);
+    i = (int)(e - (long long)j * NXG);
     const bool ii = (i >= 1 && i <= nx), jj = (j >= 1 && j <= ny);
     valid = ii || jj;  // DG_solver.f90:165 (corners are skipped)
     inner = ii && jj;
@@ -219,8 +253,14 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   const bool nd = node < NN;
   const bool act = valid && nd;
   double x[8];
+  if (s1.u0) {
+    const double dts = __dmul_rn(s1.coef, *s1.dt);
 #pragma unroll
-  for (int v = 0; v < 8; ++v) x[v] = act ? u[e * EB + v * NN + node] : 0.0;
+    for (int v = 0; v < 8; ++v) x[v] = act ? stage1_node<P>(s1, g, i, j, inner, v, node, dts) : 0.0;
+  } else {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) x[v] = act ? u[e * EB + v * NN + node] : 0.0;
+  }
   // cell averages (DG_solver.f90:177-184)
   const int k = node % N, l = node / N;
   const double w = nd ? 0.25 * dc.qw[k] * dc.qw[l] : 0.0;
@@ -294,8 +334,9 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
     const unsigned cnt = __popc(__ballot_sync(FULL_MASK, neg));
     if (lane == 0 && cnt) atomicAdd(s_cnt, (int)cnt);
   }
-  // write back state and averages of the admissible elements
-  if (valid && nd)
+  // write back state and averages of the admissible elements (the state of every element when
+  // it was formed here)
+  if ((valid || s1.u0) && act)
 #pragma unroll
     for (int v = 0; v < 8; ++v) u[e * EB + v * NN + node] = x[v];
   if (valid)
@@ -359,7 +400,7 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
                       int gate, int apply_ldf, int need_global, int ent_offset,
                       double* __restrict__ partial_sum,  // [chunks][8]
                       double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
-                      unsigned char* __restrict__ cell_ent_nan, int limit, int nchunks) {
+                      unsigned char* __restrict__ cell_ent_nan, int limit, int nchunks, Stage1Src s1) {
   using C = PPCfg<P>;
   __shared__ double s_A[C::N2 * C::N2];
   __shared__ double s_ldf[C::TE * (C::N2 + 1)];
@@ -378,7 +419,7 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
   for (int c = blockIdx.x; c < nchunks; c += gridDim.x)
     pp_avg_ldf_chunk<P, NEEDG>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
                                partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit, s_A,
-                               s_ldf, s_red, &s_cnt, run_max, run_min);
+                               s_ldf, s_red, &s_cnt, run_max, run_min, s1);
   __syncthreads();
   if (NEEDG && need_global) flush_minmax(run_max, run_min, s_red, ctrl);
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
@@ -390,7 +431,8 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
 template <int P, bool FINAL>
 __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
-                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate) {
+                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate,
+                       int stage1) {
   using C = PPCfg<P>;
   __shared__ double s_A[C::N2 * C::N2];
   __shared__ double s_ldf[C::TE * (C::N2 + 1)];
@@ -416,9 +458,10 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     }
     __syncthreads();
     const int need_global = FINAL && d.use_oedg;
+    const Stage1Src s1 = stage1 ? Stage1Src{d.u[0], d.ut[1], &d.ctrl->dt, stage1_coef(d.R)} : Stage1Src{};
     pp_avg_ldf_chunk<P, FINAL>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global, d.ent_offset,
                                d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan, !FINAL,
-                               s_A, s_ldf, s_red, &s_cnt, run_max, run_min);
+                               s_A, s_ldf, s_red, &s_cnt, run_max, run_min, s1);
     __syncthreads();
     if (need_global) flush_minmax(run_max, run_min, s_red, d.ctrl);  // per item: members differ
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
