@@ -534,21 +534,40 @@ __device__ __forceinline__ double sigsum_face(const double* Rp, const double* Lm
                                               double st_h, const double* coef) {
   constexpr int N = P + 1;
   const DegConst& dc = c_deg[P];
-  double total = 0.0;
+  // J[kk][b] = the jump of the kk-th normal derivative at face node b, formed column by column
+  // (each column of the two variable blocks is read from shared memory once)
+  double sk[N], J[N][N];
   double snk = 1.0;
-#pragma unroll 1
-  for (int kk = 0; kk <= P; ++kk) {
-    double jump[N];
 #pragma unroll
-    for (int b = 0; b < N; ++b) {
+  for (int kk = 0; kk <= P; ++kk) {
+    sk[kk] = snk;
+    snk *= sn_h;
+  }
+#pragma unroll
+  for (int b = 0; b < N; ++b) {
+    double cr[N], cl[N];
+#pragma unroll
+    for (int a = 0; a < N; ++a) {
+      cr[a] = Rp[a * sn + b * st];
+      cl[a] = Lm[a * sn + b * st];
+    }
+#pragma unroll
+    for (int kk = 0; kk <= P; ++kk) {
       double tr = 0.0, tl = 0.0;
 #pragma unroll
       for (int a = 0; a < N; ++a) {
-        tr += dc.R0[kk][a] * Rp[a * sn + b * st];
-        tl += dc.RN[kk][a] * Lm[a * sn + b * st];
+        tr += dc.R0[kk][a] * cr[a];
+        tl += dc.RN[kk][a] * cl[a];
       }
-      jump[b] = snk * tr - snk * tl;
+      J[kk][b] = sk[kk] * tr - sk[kk] * tl;
     }
+  }
+  double total = 0.0;
+#pragma unroll
+  for (int kk = 0; kk <= P; ++kk) {
+    double jump[N];
+#pragma unroll
+    for (int b = 0; b < N; ++b) jump[b] = J[kk][b];
 #pragma unroll
     for (int ll = 0; ll <= P; ++ll) {
       if (ll > P - kk) break;
@@ -569,7 +588,6 @@ __device__ __forceinline__ double sigsum_face(const double* Rp, const double* Lm
         for (int a = 0; a < N; ++a) jump[a] = nj[a];
       }
     }
-    snk *= sn_h;
   }
   return total;
 }
@@ -639,20 +657,22 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
   const int nfx = H * (W + right), nfy = W * (H + top);
   for (int it = tid; it < 8 * (nfx + nfy); it += NT) {
     const int v = it & 7, f = it >> 3;
-    if (f < nfx) {  // x face: row r, face c between columns c-1 and c of the tile
+    const bool xf = f < nfx;
+    const double* lo;  // the element before the face
+    double* dst;
+    if (xf) {  // x face: row r, face c between columns c-1 and c of the tile
       const int r = f / (W + right), c = f - r * (W + right);
-      const double* pl = s_e + ((r + 1) * RW + c) * ES + v * VS;
-      const int i = i0 + c, j = j0 + r;
-      sig_x[(((long long)(j - 1) * (nx + 1)) + (i - 1)) * 8 + v] =
-          sigsum_face<P>(pl + ES, pl, 1, P + 1, sxh, syh, s_coef);
+      lo = s_e + ((r + 1) * RW + c) * ES + v * VS;
+      dst = sig_x + (((long long)(j0 + r - 1) * (nx + 1)) + (i0 + c - 1)) * 8 + v;
     } else {  // y face: column c, face r between rows r-1 and r of the tile
       const int f2 = f - nfx;
       const int c = f2 / (H + top), r = f2 - c * (H + top);
-      const double* pb = s_e + (r * RW + c + 1) * ES + v * VS;
-      const int i = i0 + c, j = j0 + r;
-      sig_y[(((long long)(j - 1) * nx) + (i - 1)) * 8 + v] =
-          sigsum_face<P>(pb + RW * ES, pb, P + 1, 1, syh, sxh, s_coef + (P + 1) * (P + 1));
+      lo = s_e + (r * RW + c + 1) * ES + v * VS;
+      dst = sig_y + (((long long)(j0 + r - 1) * nx) + (i0 + c - 1)) * 8 + v;
     }
+    // one call site for both directions (the strides and scales select the direction)
+    *dst = sigsum_face<P>(lo + (xf ? ES : RW * ES), lo, xf ? 1 : P + 1, xf ? P + 1 : 1, xf ? sxh : syh,
+                          xf ? syh : sxh, s_coef + (xf ? 0 : (P + 1) * (P + 1)));
   }
 }
 
