@@ -627,6 +627,14 @@ struct SigLayout {
   static constexpr int DOUBLES = RW * RH * ES;
 };
 
+// 8-byte global -> shared copies that do not pass through registers (cp.async, sm_80 and later)
+__device__ __forceinline__ void cp_async8(double* dst_shared, const double* src_global) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_shared);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src_global) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <int P>
 __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, int tile_x, int tile_y,
                                                double* __restrict__ sig_x, double* __restrict__ sig_y) {
@@ -634,39 +642,50 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
   constexpr int NN = L::NN, EB = L::EB, VS = L::VS, ES = L::ES, TX = L::TX, TY = L::TY, RW = L::RW;
   constexpr int NT = 256;
   __shared__ double s_e[L::DOUBLES];  // face math reads its two variable blocks from here
+  __shared__ double s_coef[2 * (P + 1) * (P + 1)];  // x faces (h = hx), then y faces (h = hy)
   const int tid = threadIdx.x;
-  const int nx = g.nx, ny = g.ny, NXG = nx + 2;
+  const int nx = g.nx, ny = g.ny;
   const int i0 = 1 + tile_x * TX, j0 = 1 + tile_y * TY;
   const int W = min(TX, nx - i0 + 1), H = min(TY, ny - j0 + 1);
   const int right = (i0 + W - 1 == nx), top = (j0 + H - 1 == ny);
   const int cw = W + 1 + right, rh = H + 1 + top;  // staged columns i0-1 .., rows j0-1 ..
-  // stage: rect row rr = grid row j0-1+rr, rect column cc = grid column i0-1+cc
-  for (int it = tid; it < rh * cw * EB; it += NT) {
-    const int rr = it / (cw * EB), rem = it - rr * cw * EB;  // rem indexes a contiguous run of cw elements
-    const int cc = rem / EB, w = rem - cc * EB, v = w / NN, q = w - v * NN;
-    s_e[(rr * RW + cc) * ES + v * VS + q] = __ldg(u + ((long long)(j0 - 1 + rr) * NXG + (i0 - 1)) * EB + rem);
+  // stage: rect row rr = grid row j0-1+rr (a contiguous run of cw elements in u), rect column
+  // cc = grid column i0-1+cc.  The copies go straight to shared memory; the divisions are by
+  // compile-time constants.
+  {
+    const int run = cw * EB;
+    const long long row = (long long)(nx + 2) * EB;
+    const double* src = u + ((long long)(j0 - 1) * (nx + 2) + (i0 - 1)) * EB;
+    for (int rr = 0; rr < rh; ++rr, src += row) {
+      double* dst = s_e + rr * RW * ES;
+      for (int rem = tid; rem < run; rem += NT) {
+        const int cc = rem / EB, w = rem - cc * EB, v = w / NN, q = w - v * NN;
+        cp_async8(dst + cc * ES + v * VS + q, src + rem);
+      }
+    }
+    cp_async_commit();
   }
-  __syncthreads();
-  __shared__ double s_coef[2 * (P + 1) * (P + 1)];  // x faces (h = hx), then y faces (h = hy)
   if (tid < 2 * (P + 1) * (P + 1)) {
     const int d = tid / ((P + 1) * (P + 1)), r = tid - d * (P + 1) * (P + 1), n = r / (P + 1), t = r - n * (P + 1);
     s_coef[tid] = (n + t <= P) ? sigsum_coef<P>(n, t, d == 0 ? g.hx : g.hy) : 0.0;
   }
+  cp_async_wait_all();
   __syncthreads();
   const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
-  const int nfx = H * (W + right), nfy = W * (H + top);
+  const int wr = W + right, ht = H + top;  // TX and TY on interior tiles
+  const int nfx = H * wr, nfy = W * ht;
   for (int it = tid; it < 8 * (nfx + nfy); it += NT) {
     const int v = it & 7, f = it >> 3;
     const bool xf = f < nfx;
     const double* lo;  // the element before the face
     double* dst;
     if (xf) {  // x face: row r, face c between columns c-1 and c of the tile
-      const int r = f / (W + right), c = f - r * (W + right);
+      const int r = (wr == TX) ? f / TX : f / wr, c = f - r * wr;
       lo = s_e + ((r + 1) * RW + c) * ES + v * VS;
       dst = sig_x + (((long long)(j0 + r - 1) * (nx + 1)) + (i0 + c - 1)) * 8 + v;
     } else {  // y face: column c, face r between rows r-1 and r of the tile
       const int f2 = f - nfx;
-      const int c = f2 / (H + top), r = f2 - c * (H + top);
+      const int c = (ht == TY) ? f2 / TY : f2 / ht, r = f2 - c * ht;
       lo = s_e + (r * RW + c + 1) * ES + v * VS;
       dst = sig_y + (((long long)(j0 + r - 1) * nx) + (i0 + c - 1)) * 8 + v;
     }
