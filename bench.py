@@ -60,9 +60,9 @@ def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
-        return 6650.0, "fallback"
+        return 6650.0, "fallback (MEASURED_PEAKS.json absent: earlier STREAM-copy measurement on this pool)"
 
 
 # ------------------------------------------------------------------------------ clocks sampling
@@ -459,7 +459,7 @@ def run_ours(args):
                          "traffic": measured_traffic(args.workload, "residual_kernel"),
                          "kernel": "residual_kernel",
                          "algorithmic_bytes_per_launch": res_bytes, "launch_ms": t_res * 1e3,
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "peak_source": peak_kind,
                          "note": "the residual is FP64-bound in the algorithmic model (AI above the "
                                  "FP64/HBM ridge); see roofline_fp64"},
             "roofline_fp64": {"bound": "fp64", "kernel": "residual_kernel",
