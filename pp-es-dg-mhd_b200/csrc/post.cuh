@@ -38,6 +38,19 @@ struct PPCfg {
   static constexpr int TE = (PP_NT / 32) * G;                                     // elements per CTA chunk
 };
 
+// global -> shared copies that do not pass through registers (cp.async, sm_80 and later): 8 bytes,
+// or 16 bytes with both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async8(double* dst_shared, const double* src_global) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_shared);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src_global) : "memory");
+}
+__device__ __forceinline__ void cp_async16(double* dst_shared, const double* src_global) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_shared);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src_global) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <int GS>
 __device__ __forceinline__ double grp_sum(double v) {
 #pragma unroll
@@ -181,7 +194,8 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
 
 // ---------------------------------------------------------------------------------------------
 // loop 1 for one chunk of TE consecutive element blocks of the ghosted grid (one contiguous run of
-// memory).  s_A = the LDF operator in shared memory; s_red = CTA scratch (TE * 8 + 128 doubles).
+// memory).  s_A = the LDF operator in shared memory, in output-row pairs (load_ldf); s_red = CTA
+// scratch (TE * 8 + 128 doubles).
 //
 // limit = 1 fuses loop 3 for a stage without OEDG and without the entropy sum: the interior
 // elements are limited in registers before the one write-back.  The reference skips loop 3
@@ -221,14 +235,51 @@ __device__ __forceinline__ double stage1_node(const Stage1Src& s1, const Geo& g,
   return neg ? -x : x;
 }
 
-template <int P, bool NEEDG>
+// Queues this warp's elements of `chunk` into its shared buffers as one cp.async group (16-byte
+// pieces; element blocks are multiples of 16 bytes): the blocks of u, or, with a stage-1 source,
+// the blocks of u_con (bu) and k1 (bk) of the interior elements (ghost elements are formed from
+// direct loads).  bu, bk: G * EB doubles each, 16-byte aligned.
+template <int P>
+__device__ __forceinline__ void pp_prefetch(const double* __restrict__ u, const Geo& g, long long chunk,
+                                            const Stage1Src& s1, double* bu, double* bk) {
+  using C = PPCfg<P>;
+  constexpr int EB = C::EB, G = C::G, TE = C::TE, H2 = EB / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nx = g.nx, NXG = nx + 2;
+  const long long total = (long long)NXG * (g.ny + 2);
+  const long long ef = chunk * TE + warp * G;  // the warp's first element
+  const int jf = (int)(ef / NXG), if_ = (int)(ef - (long long)jf * NXG);
+#pragma unroll
+  for (int it = lane; it < G * H2; it += 32) {
+    const int k = it / H2, o = 2 * (it - k * H2);
+    const long long e = ef + k;
+    if (e >= total) continue;
+    if (!s1.u0) {
+      cp_async16(bu + k * EB + o, u + e * EB + o);
+    } else {
+      int i = if_ + k, j = jf;
+      while (i >= NXG) {
+        i -= NXG;
+        ++j;
+      }
+      if (i >= 1 && i <= nx && j >= 1 && j <= g.ny) {
+        cp_async16(bu + k * EB + o, s1.u0 + e * EB + o);
+        cp_async16(bk + k * EB + o, s1.k1 + ((long long)(j - 1) * nx + (i - 1)) * EB + o);
+      }
+    }
+  }
+  cp_async_commit();
+}
+
+template <int P, bool NEEDG, bool PF>
 __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg, const Geo& g,
                                                  Ctrl* ctrl, long long chunk, int apply_ldf, int need_global,
                                                  int ent_offset, double* __restrict__ partial_out,  // 8 doubles
                                                  double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                                                  unsigned char* __restrict__ cell_ent_nan, int limit,
                                                  const double* s_A, double* s_ldf, double* s_red, int* s_cnt,
-                                                 double* run_max, double* run_min, const Stage1Src& s1) {
+                                                 double* run_max, double* run_min, const Stage1Src& s1,
+                                                 double* bu, double* bk, long long next_chunk) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -253,7 +304,23 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   const bool nd = node < NN;
   const bool act = valid && nd;
   double x[8];
-  if (s1.u0) {
+  if (PF) {  // this chunk's blocks are in the warp's buffers (pp_prefetch)
+    const double* pu = bu + grp * EB + node;
+    const double* pk = bk + grp * EB + node;
+    if (s1.u0) {
+      const double dts = __dmul_rn(s1.coef, *s1.dt);
+#pragma unroll
+      for (int v = 0; v < 8; ++v)
+        x[v] = !act ? 0.0
+                    : (inner ? __dadd_rn(pu[v * NN], __dmul_rn(dts, pk[v * NN]))
+                             : stage1_node<P>(s1, g, i, j, false, v, node, dts));
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) x[v] = act ? pu[v * NN] : 0.0;
+    }
+    __syncwarp();  // every lane has read the buffers: queue the next chunk into them
+    if (next_chunk >= 0) pp_prefetch<P>(u, g, next_chunk, s1, bu, bk);
+  } else if (s1.u0) {
     const double dts = __dmul_rn(s1.coef, *s1.dt);
 #pragma unroll
     for (int v = 0; v < 8; ++v) x[v] = act ? stage1_node<P>(s1, g, i, j, inner, v, node, dts) : 0.0;
@@ -292,20 +359,28 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   // LDF projection of (Bx - avg, By - avg) with the dense nodal operator: this lane forms the
   // outputs at its node (rows `node` and NN + node); the inputs come from the group's lanes
   if (apply_ldf) {  // the group's (Bx, By) - avg pass through a padded per-group shared row
-    double* sb = s_ldf + (warp * G + grp) * (N2 + 1);
+    double* sb = s_ldf + (warp * G + grp) * (N2 + 2);
     if (nd) {
       sb[node] = x[4] - avg[4];
       sb[NN + node] = x[5] - avg[5];
     }
     __syncwarp();
     double ox = 0.0, oy = 0.0;
-    if (nd)
-#pragma unroll 8
-      for (int m = 0; m < N2; ++m) {
-        const double b = sb[m];
-        ox += s_A[node + N2 * m] * b;
-        oy += s_A[NN + node + N2 * m] * b;
+    if (nd) {
+      // s_A holds (row node, row NN + node) of column m as one pair at m * NN + node (load_ldf),
+      // and the input row is read two entries at a time; the sums run over m in order
+      const double2* a2 = reinterpret_cast<const double2*>(s_A) + node;
+      const double2* b2 = reinterpret_cast<const double2*>(sb);
+#pragma unroll 4
+      for (int m = 0; m < N2; m += 2) {
+        const double2 b = b2[m >> 1];
+        const double2 a0 = a2[m * NN], a1 = a2[(m + 1) * NN];
+        ox += a0.x * b.x;
+        oy += a0.y * b.x;
+        ox += a1.x * b.y;
+        oy += a1.y * b.y;
       }
+    }
     __syncwarp();  // the row is rewritten by the next chunk
     if (valid) {
       x[4] = ox + avg[4];
@@ -389,7 +464,13 @@ __device__ __forceinline__ void flush_minmax(double* run_max, double* run_min, d
 template <int P>
 __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s_A) {
   constexpr int N2 = PPCfg<P>::N2;
-  for (int it = threadIdx.x; it < N2 * N2; it += PP_NT) s_A[it] = __ldg(A + it);
+  constexpr int NN = PPCfg<P>::NN;
+  // pair (A[node][m], A[NN + node][m]) at m * NN + node; A is stored column-major (row + N2 * m)
+  for (int it = threadIdx.x; it < N2 * NN; it += PP_NT) {
+    const int m = it / NN, node = it - m * NN;
+    s_A[2 * it] = __ldg(A + node + N2 * m);
+    s_A[2 * it + 1] = __ldg(A + NN + node + N2 * m);
+  }
 }
 
 // one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once).
@@ -402,9 +483,10 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
                       double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                       unsigned char* __restrict__ cell_ent_nan, int limit, int nchunks, Stage1Src s1) {
   using C = PPCfg<P>;
-  __shared__ double s_A[C::N2 * C::N2];
-  __shared__ double s_ldf[C::TE * (C::N2 + 1)];
+  __shared__ __align__(16) double s_A[C::N2 * C::N2];
+  __shared__ __align__(16) double s_ldf[C::TE * (C::N2 + 2)];
   __shared__ double s_red[C::TE * 8 + 128];
+  __shared__ __align__(16) double s_pf[(PP_NT / 32) * 2 * C::G * C::EB];  // per warp: u (or u_con), k1
   __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
   if (threadIdx.x == 0) s_cnt = 0;
@@ -416,10 +498,18 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
     run_max[v] = -1.0e308;
     run_min[v] = 1.0e308;
   }
-  for (int c = blockIdx.x; c < nchunks; c += gridDim.x)
-    pp_avg_ldf_chunk<P, NEEDG>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
-                               partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit, s_A,
-                               s_ldf, s_red, &s_cnt, run_max, run_min, s1);
+  // the copies of a warp's next chunk are in flight while it works on this one
+  double* bu = s_pf + (threadIdx.x >> 5) * 2 * C::G * C::EB;
+  double* bk = bu + C::G * C::EB;
+  if (blockIdx.x < nchunks) pp_prefetch<P>(u, g, blockIdx.x, s1, bu, bk);
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    cp_async_wait_all();
+    __syncwarp();
+    const long long nxt = c + gridDim.x < nchunks ? (long long)c + gridDim.x : -1;
+    pp_avg_ldf_chunk<P, NEEDG, true>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
+                                     partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit,
+                                     s_A, s_ldf, s_red, &s_cnt, run_max, run_min, s1, bu, bk, nxt);
+  }
   __syncthreads();
   if (NEEDG && need_global) flush_minmax(run_max, run_min, s_red, ctrl);
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
@@ -434,8 +524,8 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate,
                        int stage1) {
   using C = PPCfg<P>;
-  __shared__ double s_A[C::N2 * C::N2];
-  __shared__ double s_ldf[C::TE * (C::N2 + 1)];
+  __shared__ __align__(16) double s_A[C::N2 * C::N2];
+  __shared__ __align__(16) double s_ldf[C::TE * (C::N2 + 2)];
   __shared__ double s_red[C::TE * 8 + 128];
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
@@ -459,9 +549,10 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     __syncthreads();
     const int need_global = FINAL && d.use_oedg;
     const Stage1Src s1 = stage1 ? Stage1Src{d.u[0], d.ut[1], &d.ctrl->dt, stage1_coef(d.R)} : Stage1Src{};
-    pp_avg_ldf_chunk<P, FINAL>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global, d.ent_offset,
-                               d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan, !FINAL,
-                               s_A, s_ldf, s_red, &s_cnt, run_max, run_min, s1);
+    pp_avg_ldf_chunk<P, FINAL, false>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global,
+                                      d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
+                                      d.cell_ent_nan, !FINAL, s_A, s_ldf, s_red, &s_cnt, run_max, run_min, s1,
+                                      nullptr, nullptr, -1);
     __syncthreads();
     if (need_global) flush_minmax(run_max, run_min, s_red, d.ctrl);  // per item: members differ
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
@@ -627,13 +718,6 @@ struct SigLayout {
   static constexpr int DOUBLES = RW * RH * ES;
 };
 
-// 8-byte global -> shared copies that do not pass through registers (cp.async, sm_80 and later)
-__device__ __forceinline__ void cp_async8(double* dst_shared, const double* src_global) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_shared);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src_global) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <int P>
 __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, int tile_x, int tile_y,
