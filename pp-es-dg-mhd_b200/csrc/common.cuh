@@ -23,6 +23,7 @@ constexpr int MAXN = MAXP + 1;
 struct DegConst {
   double qx[MAXN];          // GLL nodes
   double qw[MAXN];          // GLL weights
+  double iqw[MAXN];         // their reciprocals
   double D[MAXN * MAXN];    // nodal differentiation matrix, column-major D[i + n*j]
   double R0[MAXN][MAXN];    // R0[kk][k] = (D^kk)(0,k)    first row of D^kk
   double RN[MAXN][MAXN];    // RN[kk][k] = (D^kk)(n-1,k)  last row of D^kk
@@ -175,8 +176,9 @@ __device__ __forceinline__ double ent_of(double rho, double prs, double gamma) {
 //            inverse series (inv_series_divisor)
 //   log:     rho_hat = rho_bar / (0.5 log(zeta)/f) = (a-b) / log(a/b)
 //   1/beta_hat = ff(beta) / beta_bar = ff(beta) * inv_bb,  inv_bb = 1/beta_bar
-// and every "/ beta_bar" becomes "* inv_bb".  Results agree with the reference's expression order
-// to a few ulp; the series/log branch is decided on the same u.
+// and every "/ beta_bar" becomes "* inv_bb"; 1/(rho_a+rho_b) and 1/(beta_a+beta_b) both come from
+// the one reciprocal 1/((rho_a+rho_b)(beta_a+beta_b)).  Results agree with the reference's
+// expression order to a few ulp; the series/log branch is decided on the same u (to an ulp).
 __device__ __forceinline__ double series_divisor(double u) {
   return 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0)));
 }
@@ -197,20 +199,25 @@ __device__ __forceinline__ void ec_flux(const double* a, const double* b, double
   const double bx_bar = 0.5 * (a[4] + b[4]);
   const double by_bar = 0.5 * (a[5] + b[5]);
   const double bz_bar = 0.5 * (a[6] + b[6]);
-  const double inv_bb = 2.0 / beta_s;  // 1 / beta_bar
   const double v_sq_bar = 0.5 * ((a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) + (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]));
   const double b_sq_bar = 0.5 * ((a[4] * a[4] + a[5] * a[5] + a[6] * a[6]) + (b[4] * b[4] + b[5] * b[5] + b[6] * b[6]));
   const double bvx = 0.5 * (a[7] * a[1] + b[7] * b[1]);
   const double bvy = 0.5 * (a[7] * a[2] + b[7] * b[2]);
   const double bvz = 0.5 * (a[7] * a[3] + b[7] * b[3]);
-  // logarithmic mean of rho
-  const double rho_d = a[0] - b[0];
-  const double fr = rho_d / rho_s, ur = fr * fr;
-  const double rho_hat = (ur < 1.4e-4) ? rho_bar * inv_series_divisor(ur) : rho_d / log(a[0] / b[0]);
-  // divisor of the logarithmic mean of beta
-  const double beta_d = a[7] - b[7];
+  const double rho_d = a[0] - b[0], beta_d = a[7] - b[7];
+  // 1/rho_s and 1/beta_s from one reciprocal
+  const double r_rb = 1.0 / (rho_s * beta_s);
+  const double inv_bb = 2.0 * (rho_s * r_rb);  // 1 / beta_bar
+  const double fr = rho_d * (beta_s * r_rb), ur = fr * fr;
   const double fb = beta_d * (0.5 * inv_bb), ub = fb * fb;
-  const double ffb = (ub < 1.4e-4) ? series_divisor(ub) : 0.5 * log(a[7] / b[7]) / fb;
+  // logarithmic mean of rho and divisor of that of beta: the series forms, replaced by the
+  // logarithmic forms in the uncommon case
+  double rho_hat = rho_bar * inv_series_divisor(ur);
+  double ffb = series_divisor(ub);
+  if (ur >= 1.4e-4 || ub >= 1.4e-4) {
+    if (ur >= 1.4e-4) rho_hat = rho_d / log(a[0] / b[0]);
+    if (ub >= 1.4e-4) ffb = 0.5 * log(a[7] / b[7]) / fb;
+  }
   const double ptot = 0.5 * (b_sq_bar + rho_bar * inv_bb);
   const double ecoef = 0.5 * (ffb * inv_bb / (gamma - 1.0) - v_sq_bar);
   const double vb = vx_bar * bx_bar + vy_bar * by_bar + vz_bar * bz_bar;
@@ -239,14 +246,16 @@ __device__ __forceinline__ void ec_flux(const double* a, const double* b, double
 
 // ESPP_HLL_flux_x (DG_solver.f90:894-1071).  wl, wr: conserved states already rotated into the
 // face normal frame (swap_xy for y faces).  out[0..7] = numerical flux, out[8] = nBn,
-// out[9] = sl, out[10] = sr.  Quotients that share a denominator are formed as products with one
-// reciprocal (1/p, 1/(gamma-1), 1/(sqrt(rho_l)+sqrt(rho_r)), 1/a_form, 1/(sr-sl)); the values agree
-// with the reference's expression order to a few ulp.
-__device__ __forceinline__ void espp_hll(const double* wl, const double* wr, double gamma, double* out) {
+// out[9] = sl, out[10] = sr.  igm1 = 1/(gamma-1).  Quotients are formed as products with shared
+// reciprocals: 1/rho_l and 1/rho_r from 1/(rho_l rho_r); 1/p_l, 1/p_r and the Roe weight
+// 1/(sqrt(rho_l)+sqrt(rho_r)) from 1/((sqrt(rho_l)+sqrt(rho_r)) p_l p_r); 1/a_form; 1/(sr-sl).
+// The values agree with the reference's expression order to a few ulp.
+__device__ __forceinline__ void espp_hll(const double* wl, const double* wr, double gamma, double igm1, double* out) {
   const double rho_l = wl[0], mx_l = wl[1], my_l = wl[2], mz_l = wl[3], bx_l = wl[4], by_l = wl[5], bz_l = wl[6], e_l = wl[7];
   const double rho_r = wr[0], mx_r = wr[1], my_r = wr[2], mz_r = wr[3], bx_r = wr[4], by_r = wr[5], bz_r = wr[6], e_r = wr[7];
-  const double gm1 = gamma - 1.0, igm1 = 1.0 / gm1;
-  const double ir_l = 1.0 / rho_l, ir_r = 1.0 / rho_r;
+  const double gm1 = gamma - 1.0;
+  const double r_rho = 1.0 / (rho_l * rho_r);
+  const double ir_l = rho_r * r_rho, ir_r = rho_l * r_rho;
   const double vx_l = ir_l * mx_l, vx_r = ir_r * mx_r;
   const double vy_l = ir_l * my_l, vy_r = ir_r * my_r;
   const double vz_l = ir_l * mz_l, vz_r = ir_r * mz_r;
@@ -257,7 +266,8 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
   const double pm_l = 0.5 * bsq_l, pm_r = 0.5 * bsq_r;
   const double p_l = fmax(gm1 * (e_l - (ek_l + pm_l)), PP_EPS);
   const double p_r = fmax(gm1 * (e_r - (ek_r + pm_r)), PP_EPS);
-  const double ip_l = 1.0 / p_l, ip_r = 1.0 / p_r;
+  const double r_p = 1.0 / (p_l * p_r);
+  const double ip_l = p_r * r_p, ip_r = p_l * r_p;
   const double pt_l = p_l + pm_l, pt_r = p_r + pm_r;
   const double bu_l = bx_l * vx_l + by_l * vy_l + bz_l * vz_l;
   const double bu_r = bx_r * vx_r + by_r * vy_r + bz_r * vz_r;

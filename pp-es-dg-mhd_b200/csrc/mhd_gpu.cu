@@ -144,6 +144,7 @@ int init_device_tables(int dev) {
     for (int i = 0; i < n; ++i) {
       tabs[p].qx[i] = x[i];
       tabs[p].qw[i] = w[i];
+      tabs[p].iqw[i] = 1.0 / w[i];
     }
     for (int i = 0; i < n * n; ++i) tabs[p].D[i] = D[i];
     for (int kk = 0; kk <= p; ++kk)

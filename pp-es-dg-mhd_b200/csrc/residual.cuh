@@ -212,6 +212,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   // kinds of work balance whatever their relative cost.
   {
     constexpr int NH = L::NFX + L::NFY, NPT = TE * L::NPAIR;
+    const double igm1 = 1.0 / (gamma - 1.0);
     constexpr int THL = L::THL;
     // One call site per flux: a y face or y pair is rotated into the x frame by swap_xy (the
     // component permutation 1<->2, 4<->5, its own inverse) on the way in and out, as the
@@ -250,7 +251,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
         wl[v] = pl[sv * sl];
         wr[v] = pr[sv * sr];
       }
-      espp_hll(wl, wr, gamma, o);
+      espp_hll(wl, wr, gamma, igm1, o);
 #pragma unroll
       for (int c = 0; c < L::FW; ++c) dst[(ydir && c < 8 ? swap_xy_var(c) : c) * ostride] = o[c];  // component-major
     };
@@ -374,14 +375,14 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       if (k == 0 || k == N - 1) {
         const bool right = (k == N - 1) && (N > 1);
         const double* fr = s_fx + (((ec + (right ? 1 : 0)) * TY + er) * N + l);
-        const double c = (right ? sxh : -sxh) / dc.qw[k];
+        const double c = (right ? sxh : -sxh) * dc.iqw[k];
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
       }
       if (l == 0 || l == N - 1) {
         const bool top = (l == N - 1) && (N > 1);
         const double* fr = s_fy + (((er + (top ? 1 : 0)) * TX + ec) * N + k);
-        const double c = (top ? syh : -syh) / dc.qw[l];
+        const double c = (top ? syh : -syh) * dc.iqw[l];
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
       }
