@@ -23,9 +23,9 @@ import build as B  # noqa: E402
 
 # (TX, TY, NT, MINB, HW) per degree; set i takes candidate i of every degree
 CANDIDATES = {
-    1: [(8, 4, 128, 4, 3), (8, 4, 128, 4, 2), (8, 8, 256, 2, 6), (16, 4, 256, 2, 5)],
-    2: [(4, 4, 128, 4, 2), (4, 4, 128, 4, 3), (8, 4, 256, 2, 5), (4, 2, 128, 4, 2)],
-    3: [(4, 2, 128, 4, 3), (4, 2, 128, 4, 2), (4, 4, 256, 2, 5), (2, 4, 128, 4, 3)],
+    1: [(4, 8, 128, 4, 3), (8, 4, 128, 4, 3), (8, 8, 256, 2, 5), (16, 4, 256, 2, 5)],
+    2: [(8, 4, 256, 2, 5), (4, 4, 128, 4, 3), (8, 4, 256, 2, 4), (4, 8, 256, 2, 5)],
+    3: [(4, 4, 256, 2, 5), (2, 4, 128, 4, 3), (4, 4, 256, 2, 6), (4, 2, 128, 4, 3)],
 }
 MESHES = {1: 724, 2: 512, 3: 512}  # vortex, about 33 M DOFs each
 
