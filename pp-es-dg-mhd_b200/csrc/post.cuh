@@ -642,8 +642,10 @@ __device__ __forceinline__ double sigsum_face(const double* Rp, const double* Lm
       cr[a] = Rp[a * sn + b * st];
       cl[a] = Lm[a * sn + b * st];
     }
+    // order 0: the rows of D^0 = I pick the end nodes (the sums below give exactly these values)
+    J[0][b] = cr[0] - cl[N - 1];
 #pragma unroll
-    for (int kk = 0; kk <= P; ++kk) {
+    for (int kk = 1; kk <= P; ++kk) {
       double tr = 0.0, tl = 0.0;
 #pragma unroll
       for (int a = 0; a < N; ++a) {
