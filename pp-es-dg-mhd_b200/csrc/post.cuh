@@ -19,7 +19,11 @@
 // are butterfly reductions inside the group (every lane ends with the same value, since IEEE
 // addition, min and max are commutative), and no CTA-wide barrier sits between the steps of one
 // element.  A CTA of PP_NT threads handles a chunk of TE = (PP_NT/32) * (32/GS) consecutive
-// elements; per-chunk partial sums are formed in element order.
+// elements; per-chunk partial sums are formed in element order.  The single-instance loop-1
+// kernel is a persistent grid over the chunks in which each warp copies its elements of the next
+// chunk into shared memory (cp.async) while it works on the current one.  In the first stage of
+// a time step loop 1 also forms the stage state from u_con and k1 (Stage1Src).  The indicator
+// kernel stages each tile of elements in shared memory with cp.async, row by row.
 #pragma once
 #include "common.cuh"
 #include "misc.cuh"
