@@ -37,7 +37,6 @@ WORKLOADS = {
     "blast400_p2": ("blast", 400, 2, True, True),
     "ot64_p2": ("ot2pi", 64, 2, True, True),
 }
-KERNELS_PER_TRY_RK3 = 34  # kernel nodes of one captured try (see enqueue_try in mhd_gpu.cu)
 
 
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12  # 148 SMs x 64 FP64 FMA/clk x 2 x 1.965 GHz
@@ -391,6 +390,7 @@ def run_ours(args):
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     tries = st_run["steps"] - st0["steps"] + st_run["retries"] - st0["retries"]
+    kernels_per_try = solver.step_graph_kernels()  # kernel nodes of the captured try graph
     ms_max = max_over_ranks(dist, ms, device)
     steps_done = st_run["steps"] - st0["steps"]
 
@@ -453,7 +453,7 @@ def run_ours(args):
                        "ldf": ldf, "pp": True, "parallelism": f"replicas{ws}",
                        "l2": "inputs larger than L2 (state %.0f MB per stage buffer)" % (u0.nbytes / 1e6),
                        "tries": tries},
-            "gpu_launches": KERNELS_PER_TRY_RK3 * tries,
+            "gpu_launches": kernels_per_try * tries,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak,
                          "traffic": measured_traffic(args.workload, "residual_kernel"),

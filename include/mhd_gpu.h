@@ -194,6 +194,11 @@ int mhd_gpu_get_status(mhd_gpu_t *h, mhd_gpu_status *st);
  * keep data on the GPU, e.g. a PyTorch tensor view).  No reference counterpart. */
 int mhd_gpu_state_device_ptr(mhd_gpu_t *h, int slot, double **dptr);
 
+/* Number of kernel launches in one try of a time step: the kernel nodes of the CUDA graph that
+ * mhd_gpu_advance captured (launches that a device-side gate turns into no-ops included).
+ * MHD_ERR_STATE before the first advance.  No reference counterpart (diagnostics). */
+int mhd_gpu_step_graph_kernels(const mhd_gpu_t *h, int *n);
+
 /* ---- batches of independent instances ---------------------------------------------------- */
 
 /* No reference counterpart (the reference runs one instance per process).  A batch advances many

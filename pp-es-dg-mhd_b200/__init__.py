@@ -215,6 +215,12 @@ class DGSolver:
         _check("mhd_gpu_advance", rc, fatal_flags=raise_on_flags)
         return st.as_dict()
 
+    def step_graph_kernels(self):
+        """kernel launches in one try of a time step (the nodes of the captured step graph)"""
+        n = C.c_int()
+        _check("mhd_gpu_step_graph_kernels", self.lib.mhd_gpu_step_graph_kernels(self.h, C.byref(n)))
+        return n.value
+
     def status(self):
         st = Status()
         rc = self.lib.mhd_gpu_get_status(self.h, C.byref(st))

@@ -98,6 +98,7 @@ SIGNATURES = {
     "mhd_gpu_advance": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(Status)]),
     "mhd_gpu_get_status": (C.c_int, [_vp, C.POINTER(Status)]),
     "mhd_gpu_state_device_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_dp)]),
+    "mhd_gpu_step_graph_kernels": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "mhd_batch_create": (C.c_int, [C.POINTER(_vp)]),
     "mhd_batch_destroy": (C.c_int, [_vp]),
     "mhd_batch_add": (C.c_int, [_vp, _vp]),

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "../../include/mhd_gpu.h"
 #include "common.cuh"
@@ -53,6 +54,7 @@ struct mhd_gpu {
   Geo geo;
   // device-resident driver
   int solve_ready;
+  int graph_kernels;  // kernel nodes of the captured step graph (0 before the first capture)
   double final_T, cfl;
   int use_oedg, use_ldf, ent_offset;
   cudaGraphExec_t step_exec;
@@ -326,6 +328,20 @@ void enqueue_try(mhd_gpu* h) {
   ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R);
 }
 
+// kernel nodes of a graph (every launch of the captured try, gated ones included)
+int count_kernel_nodes(cudaGraph_t graph) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess || n == 0) return 0;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return 0;
+  int k = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
 int build_step_graph(mhd_gpu* h) {
   if (h->step_exec) {
     cudaGraphExecDestroy(h->step_exec);
@@ -336,6 +352,7 @@ int build_step_graph(mhd_gpu* h) {
   DISPATCH_P(h, enqueue_try, h);
   cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
   if (e != cudaSuccess) return MHD_ERR_CUDA;
+  h->graph_kernels = count_kernel_nodes(graph);
   e = cudaGraphInstantiate(&h->step_exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return MHD_ERR_CUDA;
@@ -838,6 +855,13 @@ int mhd_gpu_advance(mhd_gpu_t* h, long long max_steps, int check_every, mhd_gpu_
 }
 
 int mhd_gpu_step(mhd_gpu_t* h, mhd_gpu_status* st) { return mhd_gpu_advance(h, 1, 1, st); }
+
+int mhd_gpu_step_graph_kernels(const mhd_gpu_t* h, int* n) {
+  if (!h || !n) return MHD_ERR_INVALID;
+  if (!h->step_exec) return MHD_ERR_STATE;
+  *n = h->graph_kernels;
+  return MHD_OK;
+}
 
 int mhd_gpu_state_device_ptr(mhd_gpu_t* h, int slot, double** dptr) {
   if (!h || !dptr || slot < 0 || slot > h->R) return MHD_ERR_INVALID;

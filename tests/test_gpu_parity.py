@@ -240,3 +240,19 @@ def test_ot_full_run_small(pkg, ora):
     assert err.max() <= 1e-10, err
     assert abs(sg["tot_ent"] - so["tot_ent"]) <= 1e-12 * abs(so["tot_ent"])
     g.close()
+
+
+@pytest.mark.parametrize("rknstg,oedg,expect", [(3, 1, 25), (3, 0, 23), (2, 1, 19), (1, 1, 13), (5, 1, 41)])
+def test_step_graph_kernel_count(pkg, rknstg, oedg, expect):
+    """kernel launches of one captured try: 3 (step begin, re-try residual, dt) + per stage (stage
+    time, [combination for SSP-RK(5,4) stages > 1], [boundary fill before loop 1 for stages > 1],
+    loop 1, [final stage: global sums and face indicators with OEDG, limiter, entropy sum],
+    stage end, boundary fill, residual) + step end"""
+    prob = pkg.problems.make("ot2pi")
+    with pkg.DGSolver.for_problem(prob, 8, 8, 2, rknstg) as g:
+        with pytest.raises(pkg.MHDError):
+            g.step_graph_kernels()  # no graph before the first advance
+        g.upload_state(0, prob.initial_state(8, 8, 2))
+        g.solve_begin(prob.final_T, prob.cfl, oedg, 1, 0)
+        g.advance(1)
+        assert g.step_graph_kernels() == expect
