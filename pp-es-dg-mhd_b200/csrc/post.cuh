@@ -786,7 +786,8 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
 }
 
 template <int P>
-__global__ void __launch_bounds__(256, 2)
+// 3 CTAs per SM where the face math fits 80 registers (p <= 2); p = 3 needs 2 (it spills at 80)
+__global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
     pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
                      double* __restrict__ sig_x, double* __restrict__ sig_y) {
   if (!gate_open(ctrl, gate)) return;
@@ -795,7 +796,7 @@ __global__ void __launch_bounds__(256, 2)
 
 // many instances: items = every member's tiles (row-major)
 template <int P>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
     pp_sigsum_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   const int nw = *nwork, n = *ninst;
