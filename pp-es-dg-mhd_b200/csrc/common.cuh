@@ -177,7 +177,8 @@ __device__ __forceinline__ double ent_of(double rho, double prs, double gamma) {
 //   log:     rho_hat = rho_bar / (0.5 log(zeta)/f) = (a-b) / log(a/b)
 //   1/beta_hat = ff(beta) / beta_bar = ff(beta) * inv_bb,  inv_bb = 1/beta_bar
 // and every "/ beta_bar" becomes "* inv_bb"; 1/(rho_a+rho_b) and 1/(beta_a+beta_b) both come from
-// the one reciprocal 1/((rho_a+rho_b)(beta_a+beta_b)).  Results agree with the reference's
+// the one reciprocal 1/((rho_a+rho_b)(beta_a+beta_b)), and "/ (gamma-1)" is a product with
+// igm1 = 1/(gamma-1), formed once by the caller.  Results agree with the reference's
 // expression order to a few ulp; the series/log branch is decided on the same u (to an ulp).
 __device__ __forceinline__ double series_divisor(double u) {
   return 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0)));
@@ -190,7 +191,7 @@ __device__ __forceinline__ double inv_series_divisor(double u) {
 }
 
 template <int DIR>
-__device__ __forceinline__ void ec_flux(const double* a, const double* b, double gamma, double* f) {
+__device__ __forceinline__ void ec_flux(const double* a, const double* b, double igm1, double* f) {
   const double rho_s = a[0] + b[0], beta_s = a[7] + b[7];
   const double rho_bar = 0.5 * rho_s;
   const double vx_bar = 0.5 * (a[1] + b[1]);
@@ -219,7 +220,7 @@ __device__ __forceinline__ void ec_flux(const double* a, const double* b, double
     if (ub >= 1.4e-4) ffb = 0.5 * log(a[7] / b[7]) / fb;
   }
   const double ptot = 0.5 * (b_sq_bar + rho_bar * inv_bb);
-  const double ecoef = 0.5 * (ffb * inv_bb / (gamma - 1.0) - v_sq_bar);
+  const double ecoef = 0.5 * (ffb * inv_bb * igm1 - v_sq_bar);
   const double vb = vx_bar * bx_bar + vy_bar * by_bar + vz_bar * bz_bar;
   if (DIR == 0) {
     f[0] = rho_hat * vx_bar;

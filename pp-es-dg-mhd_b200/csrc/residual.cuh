@@ -276,7 +276,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
         A[v] = pA[sv * NN];
         B[v] = pB[sv * NN];
       }
-      ec_flux<0>(A, B, gamma, F);
+      ec_flux<0>(A, B, igm1, F);
       double* dst = s_pair + e * L::NPAIR + pi;  // variable-major: no bank conflicts
 #pragma unroll
       for (int v = 0; v < 8; ++v) dst[(ydir ? swap_xy_var(v) : v) * TE * L::NPAIR] = F[v];
