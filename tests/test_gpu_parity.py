@@ -256,3 +256,27 @@ def test_step_graph_kernel_count(pkg, rknstg, oedg, expect):
         g.solve_begin(prob.final_T, prob.cfl, oedg, 1, 0)
         g.advance(1)
         assert g.step_graph_kernels() == expect
+
+
+PIPELINE_FLAGS = [(3, 1, 1, 1), (3, 0, 1, 0), (3, 1, 0, 0), (3, 0, 0, 1), (1, 1, 1, 1), (2, 1, 1, 1)]
+
+
+@pytest.mark.parametrize("name,n,p", [("blast", 16, 2), ("ot2pi", 12, 3)])
+@pytest.mark.parametrize("rknstg,oedg,ldf,ent_offset", PIPELINE_FLAGS)
+def test_pipeline_flag_parity(pkg, ora, name, n, p, rknstg, oedg, ldf, ent_offset):
+    """three steps of the device time-step pipeline against the oracle for the solve flags:
+    OEDG off (the final stage limits without the indicators), LDF off, and the entropy-offset
+    limiter, whose cell entropies are formed in the same loop-1 pass that forms stage 1"""
+    prob, u0, g, o = _setup(pkg, ora, name, n, n, p, rknstg=rknstg)
+    sg = g.solve_execute(u0, prob.final_T, prob.cfl, oedg, ldf, ent_offset, max_steps=3)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, prob.cfl, oedg, ldf, ent_offset, max_steps=3)
+    assert so["status"] == 0 and sg["flags"] == 0
+    assert sg["steps"] == so["steps"] == 3 and sg["retries"] == so["retries"]
+    assert sg["num_negcell_total"] == so["num_negcell_total"]
+    assert abs(sg["t"] - so["t"]) <= 1e-14 * so["t"]
+    ug = g.download_state(0)
+    assert abs(sg["tot_ent"] - so["tot_ent"]) <= _ent_tol(ug, prob.gamma) * abs(so["tot_ent"])
+    err = rel_l1(ug[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+    assert err.max() <= TOL, err
+    g.close()
