@@ -115,3 +115,46 @@ def test_launch_then_wait_equals_advance(pkg):
         np.testing.assert_array_equal(a2.download_state(0), r2.download_state(0))
     for s in (a1, a2, r1, r2):
         s.close()
+
+
+FLAG_MIX = [  # (name, n, p, rknstg, use_oedg, use_ldf, ent_offset)
+    ("blast", 16, 2, 3, 1, 1, 1), ("blast", 12, 2, 3, 0, 1, 0), ("ot2pi", 14, 3, 3, 1, 0, 0),
+    ("rotor", 12, 1, 3, 0, 0, 1), ("ot2pi", 10, 2, 2, 1, 1, 1), ("rotor", 10, 3, 1, 1, 1, 0),
+]
+
+
+def _make_flags(pkg, name, n, p, rknstg, oedg, ldf, ent_offset):
+    prob = pkg.problems.make(name)
+    s = pkg.DGSolver.for_problem(prob, n, n, p, rknstg)
+    s.upload_state(0, prob.initial_state(n, n, p))
+    s.solve_begin(prob.final_T, prob.cfl, oedg, ldf, ent_offset)
+    return s
+
+
+def test_members_with_mixed_solve_flags_identical_to_solo_runs(pkg):
+    """members that differ in OEDG, LDF, the entropy offset and the SSP-RK scheme share a batch and
+    still compute bit for bit what they compute alone"""
+    K = 4
+    solo = []
+    for spec in FLAG_MIX:
+        s = _make_flags(pkg, *spec)
+        st = s.advance(K)
+        solo.append((s.download_state(0), st))
+        s.close()
+    with pkg.Batch() as b:
+        members = [_make_flags(pkg, *spec) for spec in FLAG_MIX]
+        for m in members:
+            b.add(m)
+        b.advance(K)
+        for m, (u_ref, st_ref) in zip(members, solo):
+            st = b.status(m)
+            assert st["retries"] == st_ref["retries"] == 0
+            assert st["steps"] == st_ref["steps"] == K
+            assert st["t"] == st_ref["t"] and st["dt_lim"] == st_ref["dt_lim"]
+            assert st["tot_ent"] == st_ref["tot_ent"]
+            assert st["num_negcell_total"] == st_ref["num_negcell_total"]
+        for m in list(members):
+            b.remove(m)
+        for m, (u_ref, _) in zip(members, solo):
+            np.testing.assert_array_equal(m.download_state(0), u_ref)
+            m.close()
