@@ -75,12 +75,13 @@ __device__ __forceinline__ double grp_max(double v) {
 }
 
 // All eight sums of a[0..7] over each group of GS lanes, in every lane of the group, by a
-// reduce-scatter (each exchange halves the values a lane carries, one lane bit per level) and an
-// all-gather: 8 + 7 exchanges at GS = 16 instead of 8 butterflies of 4.  Deterministic, and every
-// lane of a group ends with the same sums (each final sum is formed in one lane pair as x + y and
-// y + x, which IEEE addition makes equal, and gathered from one lane).
+// reduce-scatter (each exchange halves the values a lane carries, one lane bit per level: 8
+// exchanges at GS = 16 instead of 8 butterflies of 4) and an all-gather through the group's
+// shared row `row` (8 doubles).  Deterministic, and every lane of a group ends with the same sums
+// (each final sum is formed in one lane pair as x + y and y + x, which IEEE addition makes equal,
+// and read from the one copy in `row`).
 template <int GS>
-__device__ __forceinline__ void grp_sum8(double* a) {
+__device__ __forceinline__ void grp_sum8(double* a, double* row) {
   constexpr int LV = GS >= 8 ? 3 : (GS == 4 ? 2 : 1);  // halving levels
   const int lane = threadIdx.x & 31;
   constexpr int CNT = 8 >> LV;                          // values a lane keeps after them
@@ -100,18 +101,19 @@ __device__ __forceinline__ void grp_sum8(double* a) {
   for (int o = GS >> (LV + 1); o > 0; o >>= 1)
 #pragma unroll
     for (int i = 0; i < CNT; ++i) a[i] = a[i] + __shfl_xor_sync(FULL_MASK, a[i], o);
-  const int gbase = lane & ~(GS - 1);
-  double out[8];
+  // all-gather through the group's shared row: the lane that holds variables vb..vb+CNT-1 (and
+  // whose low bits are zero) writes them, every lane reads all 8
+  int vb = 0;
 #pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    int src = gbase;
+  for (int j = 0; j < LV; ++j)
+    if (lane & (GS >> (j + 1))) vb += 4 >> j;
+  if ((lane & ((GS >> LV) - 1)) == 0)
 #pragma unroll
-    for (int j = 0; j < LV; ++j)
-      if (v & (4 >> j)) src += GS >> (j + 1);
-    out[v] = __shfl_sync(FULL_MASK, a[v & (CNT - 1)], src);
-  }
+    for (int i = 0; i < CNT; ++i) row[vb + i] = a[i];
+  __syncwarp();
 #pragma unroll
-  for (int v = 0; v < 8; ++v) a[v] = out[v];
+  for (int v = 0; v < 8; ++v) a[v] = row[v];
+  __syncwarp();  // the row is rewritten next
 }
 
 __device__ __forceinline__ double node_prs(const double* x, double gamma) {
@@ -338,7 +340,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   double avg[8];
 #pragma unroll
   for (int v = 0; v < 8; ++v) avg[v] = w * x[v];
-  grp_sum8<GS>(avg);
+  grp_sum8<GS>(avg, s_ldf + (warp * G + grp) * (N2 + 2));
   // admissibility of the average (DG_solver.f90:186-193): an inadmissible element is left unwritten
   if (valid) {
     const double prs = prs_of(avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6], avg[7], gamma);
