@@ -213,7 +213,10 @@ def test_multi_step_blast_limiter_counts(pkg, ora):
 
 
 def test_retry_path(pkg, ora):
-    """an over-large CFL makes an average inadmissible; both re-try with the golden-ratio shrink"""
+    """an over-large CFL makes an average inadmissible; both re-try with the golden-ratio shrink.
+    The re-tries fall in steps 2-4 (2, 1 and 4 of them), after accepted steps, so the recomputed
+    residual of u_con reads u_con's ghost ring as the reference leaves it: filled when the solve
+    starts and not refreshed on acceptance (drive.f90:100-105, 304-311)."""
     prob, u0, g, o = _setup(pkg, ora, "blast", 16, 16, 2)
     cfl = 10.0
     sg = g.solve_execute(u0, prob.final_T, cfl, max_steps=4)
