@@ -226,9 +226,10 @@ template <int P>
 // 1 and 3 in one kernel (the stage result is discarded if an average is inadmissible)
 // s1 (time-step pipeline, stage 1 only): loop 1 forms the stage state from u0 and the stage-1
 // residual, with its ghost ring, in place of the combination and boundary-fill launches
+// entsum_later (time-step pipeline): the entropy sum is left to the stage-end launch
 void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const double* dt_ptr, double oedg_dt,
                  int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0,
-                 Stage1Src s1 = Stage1Src{}) {
+                 Stage1Src s1 = Stage1Src{}, bool entsum_later = false) {
   const int nb1 = pp_nblk_avg<P>(h);
   const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
   if (apply_oedg) {
@@ -257,7 +258,8 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
                                                    oedg_dt, ent_offset, comput_ent, h->sig_x, h->sig_y,
                                                    h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan,
                                                    h->ent_partial, accept_dst);
-  if (comput_ent) pp_entsum_kernel<<<1, 256, 0, h->stream>>>(h->ent_partial, (int)(g3.x * g3.y), h->ctrl, gate);
+  if (comput_ent && !entsum_later)
+    pp_entsum_kernel<<<1, 256, 0, h->stream>>>(h->ent_partial, (int)(g3.x * g3.y), h->ctrl, gate);
 }
 
 #define DISPATCH_P(h, fn, ...)              \
@@ -309,20 +311,23 @@ void enqueue_try(mhd_gpu* h) {
   const int R = h->R;
   ctl_step_begin<<<1, 1, 0, h->stream>>>(h->ctrl);
   launch_residual<P>(h, h->u[0], h->ut[1], ST_RECOMPUTE);
-  ctl_dt<<<1, 1, 0, h->stream>>>(h->ctrl);
+  ctl_dt_stage1<<<1, 1, 0, h->stream>>>(h->ctrl, R);  // dt, and the pseudo-time of stage 1
   // SSP-RK(2,2) and (3,3): stages after the first take their combination from the previous
   // stage's residual (next_stage_combine); SSP-RK(1,1) and (5,4) keep the separate combine
+  constexpr int EB = 8 * (P + 1) * (P + 1);
+  const long long nghost = 2LL * (h->nx + h->ny) * EB;
+  const int nseg = (int)(pp_grid_limit<P>(h).x * pp_grid_limit<P>(h).y);
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
-    ctl_stage_time<<<1, 1, 0, h->stream>>>(h->ctrl, R, s);
     // stage 1: loop 1 forms the stage state and its ghost ring (Stage1Src)
     if (s > 1 && R > 3) launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
     if (s > 1) launch_bc<P>(h, h->u[s], ST_RUN);
     const Stage1Src s1 = s == 1 ? Stage1Src{h->u[0], h->ut[1], &h->ctrl->dt, stage1_coef(R)} : Stage1Src{};
     launch_post<P>(h, s, h->use_oedg && fin, h->use_ldf, &h->ctrl->dt, 0.0, h->ent_offset, fin,
-                   fin ? h->u[0] : nullptr, ST_RUN, 1, s1);
-    ctl_stage_end<<<1, 1, 0, h->stream>>>(h->ctrl);
-    launch_bc<P>(h, h->u[s], ST_RUN);
+                   fin ? h->u[0] : nullptr, ST_RUN, 1, s1, /*entsum_later=*/true);
+    // entropy sum (final stage), stage-end decision, next stage's pseudo-time and the ghost ring
+    stage_end_bc_kernel<P><<<grid1d(nghost, 256), 256, 0, h->stream>>>(
+        h->u[s], h->geo, h->ctrl, R, fin ? 0 : s + 1, fin ? h->ent_partial : nullptr, nseg);
     launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN, fin ? StageCombine{} : next_stage_combine(h, s + 1));
   }
   ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R);

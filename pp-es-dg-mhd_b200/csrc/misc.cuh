@@ -349,10 +349,12 @@ __device__ __forceinline__ void ctl_step_end_body(Ctrl* c, int R) {
 }
 
 __global__ void ctl_step_begin(Ctrl* c) { ctl_step_begin_body(c); }
-__global__ void ctl_dt(Ctrl* c) { ctl_dt_body(c); }
-__global__ void ctl_stage_time(Ctrl* c, int R, int s) { ctl_stage_time_body(c, R, s); }
-__global__ void ctl_stage_end(Ctrl* c) { ctl_stage_end_body(c); }
 __global__ void ctl_step_end(Ctrl* c, int R) { ctl_step_end_body(c, R); }
+// the dt of the try and the pseudo-time of its first stage, in one launch
+__global__ void ctl_dt_stage1(Ctrl* c, int R) {
+  ctl_dt_body(c);
+  ctl_stage_time_body(c, R, 1);
+}
 
 // The starting control block of solve_execute (drive.f90:67-73) without a host round trip: the
 // initial post_process and residual ran just before on this stream, and their outputs (neg_avg,

@@ -962,6 +962,37 @@ __device__ __forceinline__ void pp_entsum_body(const double* __restrict__ partia
   if (tid == 0) ctrl->tot_ent = s[0];
 }
 
+// The end of a stage of the time-step pipeline in one launch over the ghost values of the stage
+// state u: block 0 forms the total entropy from the limiter's partials (final stage only:
+// ent_partial != NULL) and then, in one thread, the stage-end decision (ctl_stage_end_body) and the
+// pseudo-time of the next stage (next_stage > 0); every block fills the ghost ring of u if the
+// stage was still running when the launch began.  A block that already sees the stage abandoned
+// skips its fill, and a fill of an abandoned stage only writes scratch ghosts, so the result is
+// that of the separate launches in sequence.
+template <int P>
+__global__ void __launch_bounds__(256) stage_end_bc_kernel(double* __restrict__ u, Geo g, Ctrl* ctrl, int R,
+                                                          int next_stage, const double* __restrict__ ent_partial,
+                                                          int ent_nblk) {
+  __shared__ int s_run, s_ent;
+  bool run;
+  if (blockIdx.x == 0) {  // one read of the state for the whole block, before thread 0 updates it
+    if (threadIdx.x == 0) {
+      s_run = ctrl->state == ST_RUN;
+      s_ent = s_run && ent_partial && !ctrl->neg_avg;
+    }
+    __syncthreads();
+    run = s_run;
+    if (s_ent) pp_entsum_body(ent_partial, ent_nblk, ctrl);  // whole block
+    if (threadIdx.x == 0) {
+      ctl_stage_end_body(ctrl);
+      if (next_stage > 0) ctl_stage_time_body(ctrl, R, next_stage);
+    }
+  } else {
+    run = *reinterpret_cast<volatile const int*>(&ctrl->state) == ST_RUN;
+  }
+  if (run) bc_value<P>(u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 __global__ void __launch_bounds__(256) pp_entsum_kernel(const double* __restrict__ partial, int nblk,
                                                         Ctrl* ctrl, int gate) {
   if (!gate_open(ctrl, gate)) return;
