@@ -188,7 +188,7 @@ int full_grid(K kernel, int threads, size_t smem, int nsm) {
 }
 
 struct BatchGrids {
-  int res, cmb, bc, avg, avg_final, sig, lim;
+  int res, cmb, bc, avg, avg_final, sig, lim, seb;
 };
 
 // queried before a capture begins (the occupancy calculator is host-only work)
@@ -203,6 +203,7 @@ BatchGrids batch_grids(int nsm) {
   gr.avg_final = full_grid(pp_avg_ldf_batched<P, true>, PP_NT, 0, nsm);
   gr.sig = full_grid(pp_sigsum_batched<P>, 256, 0, nsm);
   gr.lim = full_grid(pp_limit_batched<P>, PP_NT, 0, nsm);
+  gr.seb = full_grid(stage_end_bc_batched<P>, 256, 0, nsm);
   return gr;
 }
 
@@ -219,10 +220,9 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_BEGIN, R, 0);
   residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE,
                                                               0, 0.0, 0.0);
-  ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_DT, R, 0);
+  ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_DT_STAGE1, R, 1);  // dt, and the pseudo-time of stage 1
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
-    ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_TIME, R, s);
     // stage 1: loop 1 forms the stage state and its ghost ring; SSP-RK(2,2)/(3,3): later stages
     // come from the previous residual
     if (s > 1 && R > 3)
@@ -239,9 +239,9 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
       pp_sigsum_batched<P><<<grid_sig, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);
     }
     if (fin) pp_limit_batched<P><<<grid_lim, PP_NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
-    if (fin) pp_entsum_batched<<<b->nsm, 256, 0, st>>>(in, ninst, ST_RUN);
-    ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STAGE_END, R, s);
-    bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
+    // entropy sum (final stage), stage-end decision, next stage's pseudo-time and the ghost rings
+    stage_end_bc_batched<P><<<gr.seb, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, R, fin ? 0 : s + 1,
+                                                     fin);
     // the coefficients of combine_value for SSP-RK(2,2) stage 2 and SSP-RK(3,3) stages 2, 3
     const int nxt = (!fin && (R == 2 || R == 3)) ? s + 1 : 0;
     const double ca = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.75 : 1.0 / 3.0));

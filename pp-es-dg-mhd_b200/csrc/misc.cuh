@@ -380,16 +380,17 @@ __global__ void ctl_solve_begin(Ctrl* c, double final_T, double cfl_total) {
 }
 
 // the same decisions for every instance of a batch, one thread each
-enum CtlOp : int { CTL_STEP_BEGIN = 0, CTL_DT = 1, CTL_STAGE_TIME = 2, CTL_STAGE_END = 3, CTL_STEP_END = 4 };
+enum CtlOp : int { CTL_STEP_BEGIN = 0, CTL_DT_STAGE1 = 1, CTL_STEP_END = 2 };
 __global__ void ctl_batched(const InstDesc* __restrict__ insts, const int* __restrict__ ninst, int op, int R, int s) {
   const int n = *ninst;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     Ctrl* c = insts[i].ctrl;
     switch (op) {
       case CTL_STEP_BEGIN: ctl_step_begin_body(c); break;
-      case CTL_DT: ctl_dt_body(c); break;
-      case CTL_STAGE_TIME: ctl_stage_time_body(c, R, s); break;
-      case CTL_STAGE_END: ctl_stage_end_body(c); break;
+      case CTL_DT_STAGE1:
+        ctl_dt_body(c);
+        ctl_stage_time_body(c, R, 1);
+        break;
       default: ctl_step_end_body(c, R); break;
     }
   }

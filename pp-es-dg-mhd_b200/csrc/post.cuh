@@ -12,6 +12,9 @@
 //                       scaling with its bounded re-limit loop, entropy-offset limiting, cell
 //                       entropy (chunk partials, fixed order).
 //   pp_entsum_kernel    total entropy from the partials (fixed order).
+//   stage_end_bc_kernel the end of a stage of the time-step pipeline in one launch: the entropy sum
+//                       (final stage), the stage-end decision, the next stage's pseudo-time and
+//                       the ghost fill of the stage state.
 //
 // Loops 1 and 3 work element-locally, so they map one element to a group of GS lanes of a warp,
 // one lane per GLL node, each lane holding its node's 8 variables in registers.  Loads and stores
@@ -1000,14 +1003,36 @@ __global__ void __launch_bounds__(256) pp_entsum_kernel(const double* __restrict
   pp_entsum_body(partial, nblk, ctrl);
 }
 
-__global__ void __launch_bounds__(256) pp_entsum_batched(const InstDesc* __restrict__ insts,
-                                                         const int* __restrict__ ninst, int gate) {
-  const int n = *ninst;
+// many instances: stage_end_bc_kernel for every member of a batch -- the ghost fills of all
+// members (items = every member's blocks of 256 ghost values) and, one CTA per member, the entropy
+// sum (final stage), the stage-end decision and the next stage's pseudo-time.  A fill that runs
+// after its member's decision abandoned the stage is skipped, which changes nothing (the stage's
+// state is scratch then).
+template <int P>
+__global__ void __launch_bounds__(256) stage_end_bc_batched(const InstDesc* __restrict__ insts,
+                                                           const int* __restrict__ pref, const int* __restrict__ nwork,
+                                                           const int* __restrict__ ninst, int slot, int R,
+                                                           int next_stage, int final) {
+  __shared__ int s_run, s_ent;
+  const int nw = *nwork, n = *ninst;
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const InstDesc& d = insts[it.m];
+    if (*reinterpret_cast<volatile const int*>(&d.ctrl->state) != ST_RUN) continue;
+    bc_value<P>(d.u[slot], d.g, (long long)it.local() * 256 + threadIdx.x);
+  }
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const InstDesc& d = insts[i];
-    if (!gate_open(d.ctrl, gate) || d.ctrl->neg_avg) continue;
-    pp_entsum_body(d.ent_partial, d.nseg_limit, d.ctrl);
+    __syncthreads();  // s_run and s_ent of the previous member are read
+    if (threadIdx.x == 0) {
+      s_run = d.ctrl->state == ST_RUN;
+      s_ent = s_run && final && !d.ctrl->neg_avg;
+    }
     __syncthreads();
+    if (s_ent) pp_entsum_body(d.ent_partial, d.nseg_limit, d.ctrl);  // whole block
+    if (threadIdx.x == 0) {
+      ctl_stage_end_body(d.ctrl);
+      if (next_stage > 0) ctl_stage_time_body(d.ctrl, R, next_stage);
+    }
   }
 }
 
