@@ -162,6 +162,9 @@ int init_device_tables(int dev) {
   CK(cudaFuncSetAttribute(residual_batched<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
   CK(cudaFuncSetAttribute(residual_batched<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
   CK(cudaFuncSetAttribute(residual_batched<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual_persistent<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual_persistent<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual_persistent<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
   g_dev_init[dev] = true;
   return MHD_OK;
 }
@@ -208,6 +211,29 @@ void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate, StageCom
   using L = ResLayout<P>;
   dim3 grid((h->nx + L::TX - 1) / L::TX, (h->ny + L::TY - 1) / L::TY);
   residual_kernel<P><<<grid, ResCfg<P>::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate, sc);
+}
+
+// the re-try residual of a try (gate ST_RECOMPUTE, usually closed): a persistent grid of the CTAs
+// the device holds at once
+template <int P>
+int res_resident_ctas(int dev) {
+  static int cached[kMaxDevices];
+  if (dev < 0 || dev >= kMaxDevices) return 1;
+  if (!cached[dev]) {
+    int nsm = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, residual_persistent<P>, ResCfg<P>::NT,
+                                                  ResLayout<P>::BYTES);
+    cached[dev] = std::max(1, nsm) * std::max(1, per_sm);
+  }
+  return cached[dev];
+}
+template <int P>
+void launch_residual_retry(mhd_gpu* h, const double* u, double* ut) {
+  using L = ResLayout<P>;
+  const int ntx = (h->nx + L::TX - 1) / L::TX, ntiles = ntx * ((h->ny + L::TY - 1) / L::TY);
+  residual_persistent<P><<<std::min(ntiles, res_resident_ctas<P>(h->device)), ResCfg<P>::NT, L::BYTES, h->stream>>>(
+      u, ut, h->geo, h->ctrl, ST_RECOMPUTE, ntx, ntiles);
 }
 
 template <int P>
@@ -310,7 +336,7 @@ template <int P>
 void enqueue_try(mhd_gpu* h) {
   const int R = h->R;
   ctl_step_begin<<<1, 1, 0, h->stream>>>(h->ctrl);
-  launch_residual<P>(h, h->u[0], h->ut[1], ST_RECOMPUTE);
+  launch_residual_retry<P>(h, h->u[0], h->ut[1]);
   ctl_dt_stage1<<<1, 1, 0, h->stream>>>(h->ctrl, R);  // dt, and the pseudo-time of stage 1
   // SSP-RK(2,2) and (3,3): stages after the first take their combination from the previous
   // stage's residual (next_stage_combine); SSP-RK(1,1) and (5,4) keep the separate combine

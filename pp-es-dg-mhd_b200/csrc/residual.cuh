@@ -454,6 +454,21 @@ __global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
   residual_tile<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, sc);
 }
 
+// single instance, persistent: CTA b computes tiles b, b + gridDim.x, ... (row-major, ntx per row).
+// For a launch that is usually gated off (the re-try residual of every try): a grid of resident
+// CTAs that return at once costs far less than one CTA per tile.
+template <int P>
+__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
+    residual_persistent(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
+                        int ntx, int ntiles) {
+  if (!gate_open(ctrl, gate)) return;
+  extern __shared__ __align__(16) double sm[];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    residual_tile<P>(u, ut, g, ctrl, t % ntx, t / ntx, sm, StageCombine{});
+    __syncthreads();  // the next tile reuses shared memory
+  }
+}
+
 // many instances of degree P: a persistent grid walks every member's tiles (row-major per member);
 // the state is slot `src`, the result goes to ut[dst], or (next_stage > 0) the combination of
 // stage next_stage goes to slot next_stage
