@@ -245,6 +245,23 @@ def test_ot_full_run_small(pkg, ora):
     g.close()
 
 
+def test_ot_config_full_run(pkg, ora):
+    """the reference's own CPU configuration end to end: Orszag-Tang on 64x64 quads, degree 2,
+    SSP-RK3, CFL 0.2, OEDG + LDF + positivity, to t = 0.5 (561 steps); measured agreement is
+    ~2e-15 relative L1 per variable and ~3e-16 in the total entropy"""
+    prob, u0, g, o = _setup(pkg, ora, "ot2pi", 64, 64, 2)
+    sg = g.solve_execute(u0, prob.final_T, prob.cfl)
+    o.set_state(u0[:, :, :, 1:-1, 1:-1])
+    so = o.solve(prob.final_T, prob.cfl)
+    assert so["status"] == 0 and sg["flags"] == 0 and sg["done"] == 1
+    assert sg["steps"] == so["steps"] and sg["retries"] == so["retries"]
+    assert sg["t"] == so["t"]
+    err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+    assert err.max() <= TOL, err
+    assert abs(sg["tot_ent"] - so["tot_ent"]) <= 1e-13 * abs(so["tot_ent"])
+    g.close()
+
+
 @pytest.mark.parametrize("rknstg,oedg,expect", [(3, 1, 18), (3, 0, 16), (2, 1, 14), (1, 1, 10), (5, 1, 30)])
 def test_step_graph_kernel_count(pkg, rknstg, oedg, expect):
     """kernel launches of one captured try: 3 (step begin, re-try residual, dt with the first
