@@ -85,7 +85,8 @@ struct ResLayout {
   static constexpr int O_SIG = O_PAIR + TE * NPAIR * 8;
   static constexpr int O_PT = O_SIG + TE * 2 * NN;  // total pressure p + |B|^2/2 per node
   static constexpr int O_RED = O_PT + TE * NN;
-  static constexpr int TOTAL = O_RED + 32;  // O_RED + 16 doubles also hold the pair work counter
+  static constexpr int O_DM = O_RED + 32;  // O_RED + 16 doubles also hold the pair work counter
+  static constexpr int TOTAL = O_DM + NN + N;  // D (N x N) and 1/w_k of this degree
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
   static_assert(BYTES <= 227 * 1024, "residual tile does not fit the shared memory of one CTA");
   static_assert(ResCfg<P>::NT % 32 == 0 && ResCfg<P>::NT <= 512, "whole warps, at most 16");
@@ -137,6 +138,11 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   double* s_sig = sm + L::O_SIG;
   double* s_pt = sm + L::O_PT;
   double* s_red = sm + L::O_RED;
+  // Phase 3 indexes D and 1/w by node, so a warp reads several addresses at once: a constant-
+  // memory read is replayed per distinct address, a shared-memory read is not.  Measured on B200:
+  // faster from shared memory at p = 3 (0.8 %), slower at p = 1, equal at p = 2.
+  constexpr bool DM_SHARED = (P == 3);
+  double* s_dm = sm + L::O_DM;
   int* s_next = reinterpret_cast<int*>(s_red + 16);  // next node-pair chunk of phase 2
 
   const int tid = threadIdx.x;
@@ -147,7 +153,12 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   const double gamma = g.gamma;
 
   // ---- phase 0: load the tile and its halo traces ----
+  const DegConst& dc = c_deg[P];
   if (tid == 0) *s_next = 0;
+  if (DM_SHARED && tid < NN) s_dm[tid] = dc.D[tid];
+  if (DM_SHARED && tid < N) s_dm[NN + tid] = dc.iqw[tid];
+  auto Dm = [&](int i) { return DM_SHARED ? s_dm[i] : dc.D[i]; };
+  auto iqw = [&](int i) { return DM_SHARED ? s_dm[NN + i] : dc.iqw[i]; };
   {
     constexpr int V2 = TX * EB / 2;  // double2 per tile row
     for (int it = tid; it < H * V2; it += NT) {
@@ -294,7 +305,6 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
   __syncthreads();
 
   // ---- phase 3: assemble ut per node; dt_lim per element ----
-  const DegConst& dc = c_deg[P];
   const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
   double my_dt = 1.0e300;
   for (int it = tid; it < TE * NN + TE; it += NT) {
@@ -343,12 +353,12 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       // local div B (DG_solver.f90:813)
       double dbx = 0.0, dby = 0.0;
 #pragma unroll
-      for (int r = 0; r < N; ++r) dbx += dc.D[k + N * r] * pb[4 * NN + r + N * l];
+      for (int r = 0; r < N; ++r) dbx += Dm(k + N * r) * pb[4 * NN + r + N * l];
 #pragma unroll
-      for (int m = 0; m < N; ++m) dby += pb[5 * NN + k + N * m] * dc.D[l + N * m];
+      for (int m = 0; m < N; ++m) dby += pb[5 * NN + k + N * m] * Dm(l + N * m);
       const double divB = sxh * dbx + syh * dby;
       double acc[8];
-      const double ckk = 2.0 * sxh * dc.D[k + N * k], cll = 2.0 * syh * dc.D[l + N * l];
+      const double ckk = 2.0 * sxh * Dm(k + N * k), cll = 2.0 * syh * Dm(l + N * l);
 #pragma unroll
       for (int v = 0; v < 8; ++v) acc[v] = -(ckk * F[v]) - cll * G[v] - divB * GP[v];
       // pair contributions along x (line l) and y (column k)
@@ -358,7 +368,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       for (int r = 0; r < N; ++r) {
         if (r == k) continue;
         const int pi = l * L::NPR + pair_index(max(k, r), min(k, r));
-        const double c = 2.0 * sxh * dc.D[k + N * r];
+        const double c = 2.0 * sxh * Dm(k + N * r);
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
       }
@@ -366,7 +376,7 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       for (int m = 0; m < N; ++m) {
         if (m == l) continue;
         const int pi = L::NPX + k * L::NPR + pair_index(max(l, m), min(l, m));
-        const double c = 2.0 * syh * dc.D[l + N * m];
+        const double c = 2.0 * syh * Dm(l + N * m);
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
       }
@@ -375,14 +385,14 @@ __device__ __forceinline__ void residual_tile(const double* __restrict__ u, doub
       if (k == 0 || k == N - 1) {
         const bool right = (k == N - 1) && (N > 1);
         const double* fr = s_fx + (((ec + (right ? 1 : 0)) * TY + er) * N + l);
-        const double c = (right ? sxh : -sxh) * dc.iqw[k];
+        const double c = (right ? sxh : -sxh) * iqw(k);
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
       }
       if (l == 0 || l == N - 1) {
         const bool top = (l == N - 1) && (N > 1);
         const double* fr = s_fy + (((er + (top ? 1 : 0)) * TX + ec) * N + k);
-        const double c = (top ? syh : -syh) * dc.iqw[l];
+        const double c = (top ? syh : -syh) * iqw(l);
 #pragma unroll
         for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
       }
