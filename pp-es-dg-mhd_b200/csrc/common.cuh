@@ -40,9 +40,9 @@ struct Ctrl {
   double t, dt, dt_lim, final_T, cfl_total, tot_ent;
   double t_rk[6];
   double u_avg_global[8];   // DG_solver.f90:146,228
-  double u_vari[8];         // DG_solver.f90:146,288
   unsigned long long dt_lim_bits;  // atomicMin target, bit pattern of a positive double
-  unsigned long long umax_bits[8]; // order-preserving encodings for atomicMax/atomicMin
+  unsigned long long umax_bits[8]; // max / min of the interior node values (u_vari_global,
+                                   // DG_solver.f90:287-294), order-preserving encodings
   unsigned long long umin_bits[8];
   long long steps, retries, num_negcell_total;
   long long step_limit;  // ctl_step_begin idles once steps >= step_limit

@@ -3,12 +3,15 @@
 //   pp_avg_ldf_kernel   loop 1 (DG_solver.f90:161-277): cell averages of every interior and
 //                       non-corner ghost element, admissibility of the average, the LDF projection
 //                       of (Bx,By) as one dense nodal operator, and (for OEDG) per-chunk partial
-//                       sums of the average plus max/min of the post-LDF interior values.  In the
-//                       time-step pipeline a stage without OEDG also runs loop 3 here (fused).
-//   pp_reduce_kernel    the global average sum (fixed order) and u_vari_global (DG_solver.f90:282-294):
-//                       max|u - g| = max(umax - g, g - umin) because rounding is monotone.
-//   pp_sigsum_kernel    the OEDG face jump indicators OEDG_sigsum_x/y (DG_solver.f90:295-422).
-//   pp_limit_kernel     loop 3 (DG_solver.f90:428-656): OEDG damping, Zhang-Shu positivity
+//                       sums of the average.  In the time-step pipeline a stage without OEDG also
+//                       runs loop 3 here (fused).
+//   pp_reduce_kernel    the global average sum in a fixed order (DG_solver.f90:282-286).
+//   pp_sigsum_kernel    the OEDG face jump indicators OEDG_sigsum_x/y (DG_solver.f90:295-422), and
+//                       the max and min of the post-LDF interior node values (read from the tile
+//                       it stages anyway).
+//   pp_limit_kernel     loop 3 (DG_solver.f90:428-656): OEDG damping, with u_vari_global
+//                       (DG_solver.f90:287-294) = max|u - g| = max(umax - g, g - umin) (rounding
+//                       is monotone), Zhang-Shu positivity
 //                       scaling with its bounded re-limit loop, entropy-offset limiting, cell
 //                       entropy (chunk partials, fixed order).
 //   pp_entsum_kernel    total entropy from the partials (fixed order).
@@ -287,7 +290,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
                                                  double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                                                  unsigned char* __restrict__ cell_ent_nan, int limit,
                                                  const double* s_A, double* s_ldf, double* s_red, int* s_cnt,
-                                                 double* run_max, double* run_min, const Stage1Src& s1,
+                                                 const Stage1Src& s1,
                                                  double* bu, double* bk, long long next_chunk) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
@@ -402,13 +405,6 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
 #pragma unroll
       for (int v = 0; v < 8; ++v)
         if (v % GS == node) s_red[el * 8 + v] = inner ? (g.hx * g.hy) * avg[v] : 0.0;
-    // running max and min of the post-LDF interior node values (reduced by flush_minmax)
-    if (inner && nd)
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        run_max[v] = fmax(run_max[v], x[v]);
-        run_min[v] = fmin(run_min[v], x[v]);
-      }
   }
   bool neg = false;
   if (limit) {
@@ -438,37 +434,6 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   }
 }
 
-// the CTA's running max/min of the interior node values -> ctrl->umax_bits/umin_bits
-// (max and min are exact, so the order of the reduction does not matter); resets the running values
-__device__ __forceinline__ void flush_minmax(double* run_max, double* run_min, double* s_red, Ctrl* ctrl) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    double mx = run_max[v], mn = run_min[v];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
-      mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
-    }
-    if (lane == 0) {
-      s_red[v * 8 + warp] = mx;
-      s_red[64 + v * 8 + warp] = mn;
-    }
-    run_max[v] = -1.0e308;
-    run_min[v] = 1.0e308;
-  }
-  __syncthreads();
-  if (tid < 8) {
-    double a = s_red[tid * 8], b = s_red[64 + tid * 8];
-    for (int w2 = 1; w2 < PP_NT / 32; ++w2) {
-      a = fmax(a, s_red[tid * 8 + w2]);
-      b = fmin(b, s_red[64 + tid * 8 + w2]);
-    }
-    if (a > -1.0e308) atomicMax(&ctrl->umax_bits[tid], ord_enc(a));
-    if (b < 1.0e308) atomicMin(&ctrl->umin_bits[tid], ord_enc(b));
-  }
-  __syncthreads();
-}
 
 template <int P>
 __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s_A) {
@@ -483,9 +448,9 @@ __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s
 }
 
 // one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once).
-// NEEDG: the OEDG form (need_global), with the global sums and extrema.
+// NEEDG: the OEDG form (need_global), with the per-chunk partial sums of the averages.
 template <int P, bool NEEDG>
-__global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
+__global__ void __launch_bounds__(PP_NT, PP_MINB)
     pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                       int gate, int apply_ldf, int need_global, int ent_offset,
                       double* __restrict__ partial_sum,  // [chunks][8]
@@ -501,12 +466,6 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
   if (threadIdx.x == 0) s_cnt = 0;
   if (apply_ldf) load_ldf<P>(g.ldfA, s_A);
   __syncthreads();
-  double run_max[8], run_min[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    run_max[v] = -1.0e308;
-    run_min[v] = 1.0e308;
-  }
   // the copies of a warp's next chunk are in flight while it works on this one
   double* bu = s_pf + (threadIdx.x >> 5) * 2 * C::G * C::EB;
   double* bk = bu + C::G * C::EB;
@@ -517,10 +476,9 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
     const long long nxt = c + gridDim.x < nchunks ? (long long)c + gridDim.x : -1;
     pp_avg_ldf_chunk<P, NEEDG, true>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
                                      partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit,
-                                     s_A, s_ldf, s_red, &s_cnt, run_max, run_min, s1, bu, bk, nxt);
+                                     s_A, s_ldf, s_red, &s_cnt, s1, bu, bk, nxt);
   }
   __syncthreads();
-  if (NEEDG && need_global) flush_minmax(run_max, run_min, s_red, ctrl);
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
 }
 
@@ -528,7 +486,7 @@ __global__ void __launch_bounds__(PP_NT, NEEDG ? 2 : PP_MINB)
 // final-stage form (OEDG global reductions for instances that use OEDG); the other stages fuse
 // loop 3 (limit)
 template <int P, bool FINAL>
-__global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
+__global__ void __launch_bounds__(PP_NT, FINAL ? 3 : PP_MINB)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate,
                        int stage1) {
@@ -539,12 +497,6 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
   int loaded = -1;  // member whose LDF operator s_A holds
-  double run_max[8], run_min[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    run_max[v] = -1.0e308;
-    run_min[v] = 1.0e308;
-  }
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
     const int m = it.m, chunk = it.local();
     const InstDesc& d = insts[m];
@@ -560,16 +512,15 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 2 : PP_MINB)
     const Stage1Src s1 = stage1 ? Stage1Src{d.u[0], d.ut[1], &d.ctrl->dt, stage1_coef(d.R)} : Stage1Src{};
     pp_avg_ldf_chunk<P, FINAL, false>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global,
                                       d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
-                                      d.cell_ent_nan, !FINAL, s_A, s_ldf, s_red, &s_cnt, run_max, run_min, s1,
+                                      d.cell_ent_nan, !FINAL, s_A, s_ldf, s_red, &s_cnt, s1,
                                       nullptr, nullptr, -1);
     __syncthreads();
-    if (need_global) flush_minmax(run_max, run_min, s_red, d.ctrl);  // per item: members differ
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
 }
 
 // ---------------------------------------------------------------------------------------------
-// global average (fixed-order sum of block partials) and u_vari_global.  One CTA.
+// global average (fixed-order sum of block partials).  One CTA.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void pp_reduce_body(const double* __restrict__ partial, int nblk, Ctrl* ctrl) {
   __shared__ double s[8][256];
@@ -587,12 +538,7 @@ __device__ __forceinline__ void pp_reduce_body(const double* __restrict__ partia
       for (int v = 0; v < 8; ++v) s[v][tid] = s[v][tid] + s[v][tid + w];
     __syncthreads();
   }
-  if (tid < 8) {
-    const double gsum = s[tid][0];
-    ctrl->u_avg_global[tid] = gsum;
-    const double umax = ord_dec(ctrl->umax_bits[tid]), umin = ord_dec(ctrl->umin_bits[tid]);
-    ctrl->u_vari[tid] = fmax(0.0, fmax(umax - gsum, gsum - umin));
-  }
+  if (tid < 8) ctrl->u_avg_global[tid] = s[tid][0];
 }
 
 __global__ void __launch_bounds__(256) pp_reduce_kernel(const double* __restrict__ partial, int nblk,
@@ -730,14 +676,19 @@ struct SigLayout {
 };
 
 
+// The tile's own elements also give the max and min of every variable over their nodes, merged
+// into ctrl->umax_bits / umin_bits (order-preserving encodings; max and min are exact, so neither
+// the order of the merge nor the tiling changes the result).  The atomic is skipped when the value
+// already there is not exceeded, so that most tiles issue none.
 template <int P>
-__device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, int tile_x, int tile_y,
-                                               double* __restrict__ sig_x, double* __restrict__ sig_y) {
+__device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, Ctrl* ctrl, int tile_x,
+                                               int tile_y, double* __restrict__ sig_x, double* __restrict__ sig_y) {
   using L = SigLayout<P>;
   constexpr int NN = L::NN, EB = L::EB, VS = L::VS, ES = L::ES, TX = L::TX, TY = L::TY, RW = L::RW;
   constexpr int NT = 256;
   __shared__ double s_e[L::DOUBLES];  // face math reads its two variable blocks from here
   __shared__ double s_coef[2 * (P + 1) * (P + 1)];  // x faces (h = hx), then y faces (h = hy)
+  __shared__ double s_mm[2][NT / 32][8];              // per warp: max, min of each variable
   const int tid = threadIdx.x;
   const int nx = g.nx, ny = g.ny;
   const int i0 = 1 + tile_x * TX, j0 = 1 + tile_y * TY;
@@ -766,6 +717,28 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
   }
   cp_async_wait_all();
   __syncthreads();
+  {  // extrema of the own elements: thread tid takes variable tid & 7 of elements tid/8, tid/8 + NT/8, ...
+    const int v = tid & 7;
+    double mx = -1.0e308, mn = 1.0e308;
+    for (int e = tid >> 3; e < W * H; e += NT / 8) {
+      const int r = e / W, c = e - r * W;
+      const double* src = s_e + ((r + 1) * RW + c + 1) * ES + v * VS;
+#pragma unroll
+      for (int q = 0; q < NN; ++q) {
+        mx = fmax(mx, src[q]);
+        mn = fmin(mn, src[q]);
+      }
+    }
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1) {
+      mx = fmax(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+      mn = fmin(mn, __shfl_xor_sync(FULL_MASK, mn, o));
+    }
+    if ((tid & 31) < 8) {
+      s_mm[0][tid >> 5][v] = mx;
+      s_mm[1][tid >> 5][v] = mn;
+    }
+  }
   const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
   const int wr = W + right, ht = H + top;  // TX and TY on interior tiles
   const int nfx = H * wr, nfy = W * ht;
@@ -788,6 +761,18 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
     *dst = sigsum_face<P>(lo + (xf ? ES : RW * ES), lo, xf ? 1 : P + 1, xf ? P + 1 : 1, xf ? sxh : syh,
                           xf ? syh : sxh, s_coef + (xf ? 0 : (P + 1) * (P + 1)));
   }
+  __syncthreads();
+  if (tid < 16) {  // threads 0-7: max of variable tid; 8-15: min of variable tid - 8
+    const int v = tid & 7, lo = tid >> 3;
+    double m = s_mm[lo][0][v];
+    for (int w = 1; w < NT / 32; ++w) m = lo ? fmin(m, s_mm[1][w][v]) : fmax(m, s_mm[0][w][v]);
+    unsigned long long* dst = lo ? &ctrl->umin_bits[v] : &ctrl->umax_bits[v];
+    const unsigned long long enc = ord_enc(m), cur = *reinterpret_cast<volatile unsigned long long*>(dst);
+    if (lo ? (m < 1.0e308 && enc < cur) : (m > -1.0e308 && enc > cur)) {
+      if (lo) atomicMin(dst, enc);
+      else atomicMax(dst, enc);
+    }
+  }
 }
 
 template <int P>
@@ -796,7 +781,7 @@ __global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
     pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
                      double* __restrict__ sig_x, double* __restrict__ sig_y) {
   if (!gate_open(ctrl, gate)) return;
-  pp_sigsum_tile<P>(u, g, blockIdx.x, blockIdx.y, sig_x, sig_y);
+  pp_sigsum_tile<P>(u, g, ctrl, blockIdx.x, blockIdx.y, sig_x, sig_y);
 }
 
 // many instances: items = every member's tiles (row-major)
@@ -810,7 +795,7 @@ __global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
     const int ntx = (d.g.nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX;
-    pp_sigsum_tile<P>(d.u[slot], d.g, local % ntx, local / ntx, d.sig_x, d.sig_y);
+    pp_sigsum_tile<P>(d.u[slot], d.g, d.ctrl, local % ntx, local / ntx, d.sig_x, d.sig_y);
     __syncthreads();  // the next tile reuses shared memory
   }
 }
@@ -869,7 +854,8 @@ __device__ __forceinline__ void pp_limit_segment(
       const long long fyb = ((long long)(j - 1) * nx + (i - 1)) * 8;
       const long long fyt = ((long long)j * nx + (i - 1)) * 8;
       for (int v = node; v < 8; v += GS) {
-        const double uv = ctrl->u_vari[v];
+        const double gs = ctrl->u_avg_global[v];
+        const double uv = fmax(0.0, fmax(ord_dec(ctrl->umax_bits[v]) - gs, gs - ord_dec(ctrl->umin_bits[v])));
         double dv = 0.0;
         if (uv > OEDG_EPS)
           dv = ((mx / g.hx) * (sig_x[fxl + v] + sig_x[fxl + 8 + v]) + (my / g.hy) * (sig_y[fyb + v] + sig_y[fyt + v])) / uv;
