@@ -207,7 +207,9 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
 // ---------------------------------------------------------------------------------------------
 // loop 1 for one chunk of TE consecutive element blocks of the ghosted grid (one contiguous run of
 // memory).  s_A = the LDF operator in shared memory, in output-row pairs (load_ldf); s_red = CTA
-// scratch (TE * 8 + 128 doubles).
+// scratch of TE * 8 doubles for the chunk sums, which a caller either alternates between two such
+// buffers from chunk to chunk or protects with a barrier after the call (one barrier per chunk
+// here, between the writes of s_red and the reads).
 //
 // limit = 1 fuses loop 3 for a stage without OEDG and without the entropy sum: the interior
 // elements are limited in registers before the one write-back.  The reference skips loop 3
@@ -430,7 +432,6 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
       for (int q = 0; q < ne; ++q) sacc = sacc + s_red[q * 8 + tid];
       partial_out[tid] = sacc;
     }
-    __syncthreads();  // s_red is reused by the next chunk
   }
 }
 
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
   using C = PPCfg<P>;
   __shared__ __align__(16) double s_A[C::N2 * C::N2];
   __shared__ __align__(16) double s_ldf[C::TE * (C::N2 + 2)];
-  __shared__ double s_red[C::TE * 8 + 128];
+  __shared__ double s_red[2 * C::TE * 8];  // chunk sums, two buffers used in turn
   __shared__ __align__(16) double s_pf[(PP_NT / 32) * 2 * C::G * C::EB];  // per warp: u (or u_con), k1
   __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
@@ -470,13 +471,16 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
   double* bu = s_pf + (threadIdx.x >> 5) * 2 * C::G * C::EB;
   double* bk = bu + C::G * C::EB;
   if (blockIdx.x < nchunks) pp_prefetch<P>(u, g, blockIdx.x, s1, bu, bk);
-  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+  // the chunk sums of consecutive chunks go to alternate halves of s_red: the barrier of chunk
+  // k + 1 orders the reads of chunk k before the writes of chunk k + 2
+  int half = 0;
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x, half ^= 1) {
     cp_async_wait_all();
     __syncwarp();
     const long long nxt = c + gridDim.x < nchunks ? (long long)c + gridDim.x : -1;
     pp_avg_ldf_chunk<P, NEEDG, true>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
                                      partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit,
-                                     s_A, s_ldf, s_red, &s_cnt, s1, bu, bk, nxt);
+                                     s_A, s_ldf, s_red + half * C::TE * 8, &s_cnt, s1, bu, bk, nxt);
   }
   __syncthreads();
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
@@ -493,7 +497,7 @@ __global__ void __launch_bounds__(PP_NT, FINAL ? 3 : PP_MINB)
   using C = PPCfg<P>;
   __shared__ __align__(16) double s_A[C::N2 * C::N2];
   __shared__ __align__(16) double s_ldf[C::TE * (C::N2 + 2)];
-  __shared__ double s_red[C::TE * 8 + 128];
+  __shared__ double s_red[C::TE * 8];  // chunk sums (the loop's barriers protect it)
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
   int loaded = -1;  // member whose LDF operator s_A holds
