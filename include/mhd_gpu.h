@@ -298,13 +298,18 @@ int mhd_server_destroy(mhd_server_t *s);
  *       ([ny+2][nx+2][8][(p+1)^2] doubles, the layout mhd_gpu_state_device_ptr exposes);
  *   ut  device pointer, [ny][nx][8][(p+1)^2] doubles, written;
  *   dt_lim  host pointer (may be NULL); when given, the call waits for the stream.
+ * u and ut must both start on a 16-byte boundary (the kernel moves whole element blocks with
+ * 16-byte loads and stores) and must not overlap; a pointer that breaks either rule is rejected
+ * with MHD_ERR_INVALID before the GPU is touched.
  * The call allocates nothing: its only scratch (the dt_lim reduction cell and status words) is a
  * 4 KiB static device array inside the library, which every GPU that loads the library holds
  * until the process exits.  All calls share that array and it keeps the last call's contents;
  * the reduction cell is reset at the start of every call, and calls that overlap on the GPU
  * (different streams or host threads at the same time) race on it.
  * The first call on a device sets that device up (constant tables, kernel attributes and the
- * address of the static array); make that first call before any stream capture.
+ * address of the static array); make that first call before any stream capture.  That set-up is
+ * kept for the life of the process, like every handle's device set-up: the library must not be
+ * used across a cudaDeviceReset of its device.
  * Limits: px = py = p in 1..3, 2 <= nx, ny <= 4096; anything larger or any other argument out of
  * range is rejected with MHD_ERR_UNSUPPORTED / MHD_ERR_INVALID before touching the GPU.
  * stream: a cudaStream_t (NULL = the legacy default stream). */

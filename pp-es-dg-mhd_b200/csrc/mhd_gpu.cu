@@ -939,6 +939,14 @@ extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, 
                                               const double* u, double* ut, double* dt_lim, void* stream) {
   if (!u || !ut || !(hx > 0.0) || !(hy > 0.0) || !(gamma > 1.0) || nx < 2 || ny < 2) return MHD_ERR_INVALID;
   if (p < 1 || p > MAXP || nx > kNoAllocMaxCells || ny > kNoAllocMaxCells) return MHD_ERR_UNSUPPORTED;
+  // the kernel moves tile rows with 16-byte loads and stores: both arrays must start on a 16-byte
+  // boundary (a misaligned access would fault and lose the CUDA context), and ut must not overlap u
+  // (tiles read neighbour traces of u while other tiles write ut)
+  const uintptr_t ua = reinterpret_cast<uintptr_t>(u), ta = reinterpret_cast<uintptr_t>(ut);
+  if ((ua | ta) & 15) return MHD_ERR_INVALID;
+  const uintptr_t eb_bytes = sizeof(double) * 8 * (uintptr_t)(p + 1) * (p + 1);
+  const uintptr_t u_end = ua + eb_bytes * (uintptr_t)(nx + 2) * (ny + 2), t_end = ta + eb_bytes * (uintptr_t)nx * ny;
+  if (ua < t_end && ta < u_end) return MHD_ERR_INVALID;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return MHD_ERR_INVALID;

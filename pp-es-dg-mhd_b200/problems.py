@@ -43,10 +43,11 @@ def gll_nodes(p):
     return x, w
 
 
-def node_coords(nx, ny, p, domain):
-    """xx(p+1, nx), yy(p+1, ny) exactly as init_DG_solver computes them (DG_solver.f90:93-106)."""
+def node_coords(nx, ny, p, domain, nodes=None):
+    """xx(p+1, nx), yy(p+1, ny) exactly as init_DG_solver computes them (DG_solver.f90:93-106).
+    nodes: the p+1 GLL nodes to use (default: the library's tables)."""
     left, right, bottom, top = domain
-    q, _ = gll_nodes(p)
+    q = gll_nodes(p)[0] if nodes is None else np.asarray(nodes, dtype=np.float64)
     hx = (right - left) / nx
     hy = (top - bottom) / ny
     i = np.arange(1, nx + 1)
@@ -180,9 +181,11 @@ class Problem:
             return ids["blast"], [c[0], c[1]]
         return ids[self.name], [self.params.get("amp", 1.0)]
 
-    def initial_state(self, nx, ny, p):
-        """u(8, p+1, p+1, nx+2, ny+2) Fortran order, interior from the IC, ghost ring NaN."""
-        xx, yy = node_coords(nx, ny, p, self.domain)
+    def initial_state(self, nx, ny, p, nodes=None):
+        """u(8, p+1, p+1, nx+2, ny+2) Fortran order, interior from the IC, ghost ring NaN.
+        nodes: the p+1 GLL nodes to evaluate at (default: the library's tables; a caller that must
+        not load the library passes its own, e.g. the CPU baseline)."""
+        xx, yy = node_coords(nx, ny, p, self.domain, nodes)
         n = p + 1
         X = np.broadcast_to(xx[:, None, :, None], (n, n, nx, ny))
         Y = np.broadcast_to(yy[None, :, None, :], (n, n, nx, ny))

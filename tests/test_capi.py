@@ -113,3 +113,21 @@ def test_tuned_header_defines_every_degree():
         assert m, p
         tx, ty, nt, minb, hw = map(int, m.groups())
         assert nt % 32 == 0 and 1 <= hw <= nt // 32
+
+
+def test_noalloc_rejects_misaligned_and_overlapping_buffers_on_the_host(pkg):
+    """mhd_gpu_semidiscretize_noalloc checks its caller's pointers before any CUDA call: the
+    pointers below are never dereferenced (no GPU here)."""
+    lib = pkg.capi.load()
+    base = 1 << 24
+    bad = pkg.capi.MHD_ERR_INVALID
+    # 8-byte aligned but not 16-byte aligned: an offset into a caller's own pool
+    assert lib.mhd_gpu_semidiscretize_noalloc(2, 8, 8, 0.1, 0.1, 1.4, C.c_void_p(base + 8),
+                                              C.c_void_p(base + (1 << 20)), None, None) == bad
+    assert lib.mhd_gpu_semidiscretize_noalloc(2, 8, 8, 0.1, 0.1, 1.4, C.c_void_p(base),
+                                              C.c_void_p(base + (1 << 20) + 8), None, None) == bad
+    # ut overlapping u (either order)
+    assert lib.mhd_gpu_semidiscretize_noalloc(2, 8, 8, 0.1, 0.1, 1.4, C.c_void_p(base),
+                                              C.c_void_p(base + 4096), None, None) == bad
+    assert lib.mhd_gpu_semidiscretize_noalloc(2, 8, 8, 0.1, 0.1, 1.4, C.c_void_p(base + 4096),
+                                              C.c_void_p(base), None, None) == bad
