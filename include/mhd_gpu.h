@@ -170,6 +170,10 @@ int mhd_gpu_semidiscretize(mhd_gpu_t *h, int ut_stage, int slot, double *dt_lim)
  * (drive.f90:130-275): writes the interior of uRK_con(:,stage). */
 int mhd_gpu_rk_combine(mhd_gpu_t *h, int stage, double dt);
 
+/* The acceptance of a step (drive.f90:304-311): u_con = uRK_con(:,rknstg) on the interior
+ * elements; u_con's ghost ring is left as it was, as in the reference. */
+int mhd_gpu_rk_accept(mhd_gpu_t *h);
+
 /* ---- device-resident solve_execute (drive.f90:32-343) ----------------------------------- */
 
 /* Prologue of solve_execute after Init_handle filled u_con (drive.f90:67-75): BC,
@@ -188,6 +192,49 @@ int mhd_gpu_advance(mhd_gpu_t *h, long long max_steps, int check_every, mhd_gpu_
 
 /* Current driver status without advancing. */
 int mhd_gpu_get_status(mhd_gpu_t *h, mhd_gpu_status *st);
+
+/* ---- driver log ------------------------------------------------------------------------- */
+
+/* What solve_execute reports while it runs, recorded on the device by the device-resident driver so
+ * that a host that polls only every few steps still sees every stage: per stage the PP-limited
+ * cell count it prints (drive.f90:292-294) or the inadmissible average that abandons the try
+ * (drive.f90:285-289), per accepted step the (t, tot_ent) pair it appends to its entropy log
+ * (drive.f90:314), and the initial state's pair (drive.f90:74). */
+#define MHD_LOG_STAGE 1
+#define MHD_LOG_STEP 2
+typedef struct mhd_log_entry {
+  long long seq;        /* running record number, from 0 at solve_begin                       */
+  long long step;       /* time step (time_step_num, 1-based; 0 = the initial state)          */
+  int kind;             /* MHD_LOG_STAGE or MHD_LOG_STEP                                      */
+  int stage;            /* RK stage (stage records; step records: rknstg)                     */
+  int try_num;          /* try of the step (1 = first; the stage records of a re-try carry 2+) */
+  int num_negcell;      /* PP-limited cells of the stage                                      */
+  int neg_avg;          /* 1: inadmissible average, the try was abandoned                      */
+  int flags;            /* MHD_FLAG_* bits after the record                                   */
+  double t;             /* stage: its pseudo-time t_RK(s); step: the time reached             */
+  double dt;            /* dt of the try                                                      */
+  double dt_lim;        /* step records: dt_lim of the last residual; stage records: NaN      */
+  double tot_ent;       /* step records: total entropy of the accepted state                  */
+  double rho_min, p_min;/* diagnostics: min nodal density and pressure of the stage state      */
+  double total[8];      /* diagnostics: sum over interior nodes of (hx*hy/4)*w_k*w_l*u, i.e. the
+                           domain integrals of rho, m, B, E by the quadrature of the cell
+                           averages (DG_solver.f90:177-184); NaN without diagnostics          */
+} mhd_log_entry;
+
+/* Keep a log of `capacity` records on the device (0 = no log, the default), drained to the host at
+ * every poll of mhd_gpu_advance.  diagnostics != 0 adds, after every completed stage, one kernel
+ * that fills rho_min, p_min and total[] of the stage record (and of the step record from its final
+ * stage): the invariants the method promises (positivity after every stage, conservation) can
+ * then be checked on the device's own output.  Without it the log costs one thread's writes per
+ * stage.  Takes effect from the next mhd_gpu_solve_begin or advance (the step graph is
+ * re-captured).  Members of a batch log stage and step records, without diagnostics. */
+int mhd_gpu_set_log(mhd_gpu_t *h, int capacity, int diagnostics);
+
+/* Up to `cap` of the oldest records not yet read, removed from the log; *n = how many were copied
+ * (out == NULL: how many are waiting).  *dropped (may be NULL) = records lost because the device
+ * ring filled between two drains.  MHD_ERR_STATE without a log.  For a batch member, call between
+ * batch rounds. */
+int mhd_gpu_read_log(mhd_gpu_t *h, mhd_log_entry *out, int cap, int *n, long long *dropped);
 
 /* Device address of a state slot in the library's element-blocked layout
  * [ (ny+2) rows ][ (nx+2) elements ][ 8 variables ][ (px+1)*(py+1) nodes ]  (for callers that

@@ -12,6 +12,7 @@ include/mhd_gpu.h:
       DG_solver.f90:663
     BC_handle(u, ...)            drive.f90:25             DGSolver.apply_bc(slot)
     stage update                 drive.f90:130-275        DGSolver.rk_combine(stage, dt)
+    step acceptance              drive.f90:304-311        DGSolver.rk_accept()
     solve_execute(final_T, CFL, use_oedg, use_LDF,        DGSolver.solve_execute(...)
                   ent_offset)    drive.f90:32
     finalize_DG_solver           DG_solver.f90:109        DGSolver.close()
@@ -195,6 +196,10 @@ class DGSolver:
     def rk_combine(self, stage, dt):
         _check("mhd_gpu_rk_combine", self.lib.mhd_gpu_rk_combine(self.h, stage, float(dt)))
 
+    def rk_accept(self):
+        """u_con = uRK_con(:, rknstg) on the interior (drive.f90:304-311)"""
+        _check("mhd_gpu_rk_accept", self.lib.mhd_gpu_rk_accept(self.h))
+
     # -------------------------------------------------------------------------- driver
     def solve_begin(self, final_T, cfl, use_oedg=True, use_ldf=True, ent_offset=False):
         te, dl = C.c_double(), C.c_double()
@@ -220,6 +225,19 @@ class DGSolver:
         n = C.c_int()
         _check("mhd_gpu_step_graph_kernels", self.lib.mhd_gpu_step_graph_kernels(self.h, C.byref(n)))
         return n.value
+
+    def set_log(self, capacity=4096, diagnostics=False):
+        """keep the driver log on the device (mhd_gpu_set_log); capacity 0 turns it off"""
+        _check("mhd_gpu_set_log", self.lib.mhd_gpu_set_log(self.h, int(capacity), int(diagnostics)))
+
+    def read_log(self):
+        """(records, dropped): every log record not yet read, oldest first, as dicts (the stage
+        prints of drive.f90:285-294 and the (t, tot_ent) log of drive.f90:74,314)"""
+        n, dropped = C.c_int(), C.c_longlong()
+        _check("mhd_gpu_read_log", self.lib.mhd_gpu_read_log(self.h, None, 0, C.byref(n), C.byref(dropped)))
+        arr = (capi.LogEntry * max(1, n.value))()
+        _check("mhd_gpu_read_log", self.lib.mhd_gpu_read_log(self.h, arr, n.value, C.byref(n), C.byref(dropped)))
+        return [arr[i].as_dict() for i in range(n.value)], dropped.value
 
     def status(self):
         st = Status()

@@ -36,6 +36,22 @@ class Status(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
 
 
+class LogEntry(C.Structure):
+    """mhd_log_entry"""
+    _fields_ = [("seq", C.c_longlong), ("step", C.c_longlong), ("kind", C.c_int), ("stage", C.c_int),
+                ("try_num", C.c_int), ("num_negcell", C.c_int), ("neg_avg", C.c_int), ("flags", C.c_int),
+                ("t", C.c_double), ("dt", C.c_double), ("dt_lim", C.c_double), ("tot_ent", C.c_double),
+                ("rho_min", C.c_double), ("p_min", C.c_double), ("total", C.c_double * 8)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "total"}
+        d["total"] = list(self.total)
+        return d
+
+
+LOG_STAGE, LOG_STEP = 1, 2
+
+
 class Request(C.Structure):
     """mhd_request"""
     _fields_ = [("id", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("p", C.c_int),
@@ -93,6 +109,7 @@ SIGNATURES = {
                                        _ip, _ip, _dp]),
     "mhd_gpu_semidiscretize": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
     "mhd_gpu_rk_combine": (C.c_int, [_vp, C.c_int, C.c_double]),
+    "mhd_gpu_rk_accept": (C.c_int, [_vp]),
     "mhd_gpu_solve_begin": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "mhd_gpu_step": (C.c_int, [_vp, C.POINTER(Status)]),
     "mhd_gpu_advance": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(Status)]),
@@ -118,6 +135,9 @@ SIGNATURES = {
     "mhd_server_destroy": (C.c_int, [_vp]),
     "mhd_gpu_download_avg_primitive": (C.c_int, [_vp, C.POINTER(C.c_float), _dp, _dp]),
     "mhd_gpu_init_problem": (C.c_int, [_vp, C.c_int, _dp, C.c_int]),
+    "mhd_gpu_set_log": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "mhd_gpu_read_log": (C.c_int, [_vp, C.POINTER(LogEntry), C.c_int, C.POINTER(C.c_int),
+                                   C.POINTER(C.c_longlong)]),
     "mhd_gpu_semidiscretize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                                  C.c_double, _vp, _vp, _dp, _vp]),
 }

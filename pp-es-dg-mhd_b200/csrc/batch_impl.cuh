@@ -75,6 +75,8 @@ InstDesc make_desc(const mhd_gpu* h) {
     d.ut[s] = h->ut[s];
   }
   d.u_avg = h->u_avg;
+  d.log = h->log;
+  d.log_cap = h->log_cap;
   d.sig_x = h->sig_x;
   d.sig_y = h->sig_y;
   d.partial = h->partial;

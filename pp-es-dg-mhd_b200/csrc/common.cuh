@@ -57,7 +57,44 @@ struct Ctrl {
   int pp_relimit;
   int pending_dtlim; // a residual wrote dt_lim_bits that is not yet decoded
   int pad_[2];
+  long long log_seq; // records written to the driver log so far (LogEntry)
 };
+
+// One record of the device-resident driver's log: per stage what drive.f90:285-294 prints (the
+// PP-limited cell count, an abandoned stage), per accepted step what drive.f90:314 appends (t and
+// the total entropy).  The public struct mhd_log_entry (mhd_gpu.h) has the same layout.  The
+// diagnostic fields (rho_min, p_min, total) are NaN unless the instance runs the stage diagnostics.
+struct LogEntry {
+  long long seq;       // running record number
+  long long step;      // time step (1-based; 0 = the initial state)
+  int kind;            // LOG_STAGE or LOG_STEP
+  int stage;           // RK stage (stage records)
+  int try_num;         // try of the step (1 = first)
+  int num_negcell;     // PP-limited cells of the stage (stage records)
+  int neg_avg;         // the stage had an inadmissible average and the try was abandoned
+  int flags;           // MHD_FLAG_* bits after the record
+  double t;            // stage: its pseudo-time t_RK(s); step: the time reached
+  double dt;           // dt of the try
+  double dt_lim;       // step records: dt_lim of the last residual
+  double tot_ent;      // step records: total entropy of the accepted state
+  double rho_min, p_min;  // minimum nodal density and pressure of the stage state
+  double total[8];        // sum over interior nodes of (hx hy / 4) w_k w_l u: the domain integrals
+};
+enum LogKind : int { LOG_STAGE = 1, LOG_STEP = 2 };
+
+// The next record of a log ring of `cap` records (nullptr if the instance keeps no log); its
+// diagnostic fields start as NaN.  Single thread.
+__device__ __forceinline__ LogEntry* log_next(LogEntry* log, int cap, Ctrl* c) {
+  if (!log || cap <= 0) return nullptr;
+  const long long s = c->log_seq;
+  c->log_seq = s + 1;
+  LogEntry* e = log + (s % cap);
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  e->seq = s;
+  e->rho_min = e->p_min = nan;
+  for (int v = 0; v < 8; ++v) e->total[v] = nan;
+  return e;
+}
 
 // Per-instance geometry passed by value.
 struct Geo {
@@ -83,9 +120,12 @@ struct InstDesc {
   double* cell_ent_FV;
   unsigned char* cell_ent_nan;
   Ctrl* ctrl;
+  LogEntry* log;   // driver log ring (nullptr: none)
+  int log_cap;
   int use_oedg, use_ldf, ent_offset, R;
   int nblk_avg;    // pp_avg_ldf chunks of this instance (partial sums)
   int nseg_limit;  // pp_limit segments of this instance (entropy partials)
+  int pad_;
 };
 
 // Batched kernels see a group's work of one kind as the concatenation of every member's items;

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstddef>
 #include <cstdlib>
 #include <mutex>
 #include <new>
@@ -58,6 +59,15 @@ struct mhd_gpu {
   double final_T, cfl;
   int use_oedg, use_ldf, ent_offset;
   cudaGraphExec_t step_exec;
+  // driver log (mhd_gpu_set_log): a device ring of log_cap records, drained into log_host
+  LogEntry* log;
+  int log_cap;
+  int diag;                    // run the stage diagnostics kernel after every stage
+  double* diag_part;           // its block partials, followed by its ticket counter
+  void* log_block;
+  long long log_host_seq;      // records copied to the host so far
+  long long log_dropped;       // records overwritten in the ring before they were copied
+  std::vector<LogEntry>* log_host;
 };
 
 namespace {
@@ -288,6 +298,16 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
     pp_entsum_kernel<<<1, 256, 0, h->stream>>>(h->ent_partial, (int)(g3.x * g3.y), h->ctrl, gate);
 }
 
+// stage diagnostics of state u into the newest log record
+template <int P>
+void launch_diag(mhd_gpu* h, const double* u, int gate) {
+  const long long E = (long long)h->nx * h->ny;
+  const int nb = (int)std::min<long long>(DIAG_MAX_BLOCKS, std::max<long long>(1, E / 16));
+  stage_diag_kernel<P><<<nb, 256, 0, h->stream>>>(u, h->geo, h->ctrl, gate, h->diag_part,
+                                                   reinterpret_cast<unsigned int*>(h->diag_part + 10 * DIAG_MAX_BLOCKS),
+                                                   h->log, h->log_cap);
+}
+
 #define DISPATCH_P(h, fn, ...)              \
   do {                                      \
     switch ((h)->p) {                       \
@@ -300,6 +320,33 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
 int read_ctrl(mhd_gpu* h) {
   CK(cudaMemcpyAsync(h->ctrl_host, h->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return MHD_OK;
+}
+
+// Copy the log records written since the last drain from the device ring to the host buffer.
+// Needs a fresh ctrl_host (read_ctrl) and an idle stream.  Records the ring overwrote before they
+// could be copied are counted in log_dropped.
+int drain_log(mhd_gpu* h) {
+  if (!h->log) return MHD_OK;
+  const long long dev_seq = h->ctrl_host->log_seq;
+  long long from = h->log_host_seq;
+  if (dev_seq <= from) return MHD_OK;
+  if (dev_seq - from > h->log_cap) {
+    h->log_dropped += dev_seq - from - h->log_cap;
+    from = dev_seq - h->log_cap;
+  }
+  const long long cnt = dev_seq - from;
+  std::vector<LogEntry>& out = *h->log_host;
+  const size_t at = out.size();
+  out.resize(at + (size_t)cnt);
+  const long long first = from % h->log_cap;
+  const long long run1 = std::min<long long>(cnt, h->log_cap - first);
+  CK(cudaMemcpyAsync(out.data() + at, h->log + first, sizeof(LogEntry) * run1, cudaMemcpyDeviceToHost, h->stream));
+  if (cnt > run1)
+    CK(cudaMemcpyAsync(out.data() + at + run1, h->log, sizeof(LogEntry) * (cnt - run1), cudaMemcpyDeviceToHost,
+                       h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->log_host_seq = dev_seq;
   return MHD_OK;
 }
 
@@ -353,10 +400,11 @@ void enqueue_try(mhd_gpu* h) {
                    fin ? h->u[0] : nullptr, ST_RUN, 1, s1, /*entsum_later=*/true);
     // entropy sum (final stage), stage-end decision, next stage's pseudo-time and the ghost ring
     stage_end_bc_kernel<P><<<grid1d(nghost, 256), 256, 0, h->stream>>>(
-        h->u[s], h->geo, h->ctrl, R, fin ? 0 : s + 1, fin ? h->ent_partial : nullptr, nseg);
+        h->u[s], h->geo, h->ctrl, R, s, fin ? 0 : s + 1, fin ? h->ent_partial : nullptr, nseg, h->log, h->log_cap);
+    if (h->diag) launch_diag<P>(h, h->u[s], ST_RUN);
     launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN, fin ? StageCombine{} : next_stage_combine(h, s + 1));
   }
-  ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R);
+  ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R, h->log, h->log_cap);
 }
 
 // kernel nodes of a graph (every launch of the captured try, gated ones included)
@@ -401,6 +449,9 @@ void free_all(mhd_gpu* h) {
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaStream_t fs = h->own_stream;  // a stream-ordered free back into the device pool
   if (h->block && h->owns_block) cudaFreeAsync(h->block, fs);
+  if (h->log_block) cudaFreeAsync(h->log_block, fs);
+  delete h->log_host;
+  h->log_host = nullptr;
   if (fs) {
     cudaStreamSynchronize(fs);
     cudaStreamDestroy(fs);
@@ -793,6 +844,18 @@ int mhd_gpu_rk_combine(mhd_gpu_t* h, int stage, double dt) {
   return MHD_OK;
 }
 
+int mhd_gpu_rk_accept(mhd_gpu_t* h) {
+  int rc = enter(h);
+  if (rc) return rc;
+  // the interior rows of uRK(:,rknstg) into u_con, ghost ring untouched (drive.f90:304-311): one
+  // strided copy, a row of nx element blocks per grid row
+  const size_t row = sizeof(double) * (size_t)h->eb * h->nx, pitch = sizeof(double) * (size_t)h->eb * (h->nx + 2);
+  const size_t first = (size_t)h->eb * (h->nx + 2 + 1);  // element (1, 1)
+  CK(cudaMemcpy2DAsync(h->u[0] + first, pitch, h->u[h->R] + first, pitch, row, h->ny, cudaMemcpyDeviceToDevice,
+                       h->stream));
+  return MHD_OK;
+}
+
 int mhd_gpu_solve_begin(mhd_gpu_t* h, double final_T, double cfl, int use_oedg, int use_ldf, int ent_offset,
                         double* tot_ent, double* dt_lim) {
   int rc = enter(h);
@@ -829,6 +892,14 @@ int mhd_gpu_solve_begin(mhd_gpu_t* h, double final_T, double cfl, int use_oedg, 
   c.step_limit = 0x7fffffffffffffffLL;
   *h->ctrl_host = c;
   CK(cudaMemcpyAsync(h->ctrl, h->ctrl_host, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
+  if (h->log) {  // a new run starts a new log: its first record is the initial state (drive.f90:74)
+    h->log_host->clear();
+    h->log_host_seq = 0;
+    h->log_dropped = 0;
+    ctl_log_initial<<<1, 1, 0, h->stream>>>(h->ctrl, h->log, h->log_cap);
+    if (h->diag) DISPATCH_P(h, launch_diag, h, h->u[0], GATE_ALWAYS);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(h->stream));
   if (h->step_exec) {  // the step graph is (re)captured lazily by the first advance
     cudaGraphExecDestroy(h->step_exec);
@@ -878,6 +949,8 @@ int mhd_gpu_advance(mhd_gpu_t* h, long long max_steps, int check_every, mhd_gpu_
     for (int b = 0; b < batch; ++b) CK(cudaGraphLaunch(h->step_exec, h->stream));
     rc = read_ctrl(h);
     if (rc) return rc;
+    rc = drain_log(h);
+    if (rc) return rc;
   }
   fill_status(h, st);
   set_step_limit(h, 0x7fffffffffffffffLL);
@@ -891,6 +964,74 @@ int mhd_gpu_step_graph_kernels(const mhd_gpu_t* h, int* n) {
   if (!h || !n) return MHD_ERR_INVALID;
   if (!h->step_exec) return MHD_ERR_STATE;
   *n = h->graph_kernels;
+  return MHD_OK;
+}
+
+static_assert(sizeof(LogEntry) == sizeof(mhd_log_entry), "log record layouts differ");
+static_assert(offsetof(LogEntry, total) == offsetof(mhd_log_entry, total), "log record layouts differ");
+
+int mhd_gpu_set_log(mhd_gpu_t* h, int capacity, int diagnostics) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (capacity < 0 || capacity > (1 << 24)) return MHD_ERR_INVALID;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->log_block) {
+    CK(cudaFreeAsync(h->log_block, h->stream));
+    h->log_block = nullptr;
+  }
+  h->log = nullptr;
+  h->diag_part = nullptr;
+  h->log_cap = 0;
+  h->diag = 0;
+  if (h->step_exec) {  // the step graph is re-captured with (or without) the log by the next advance
+    cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+  }
+  if (capacity == 0) {
+    delete h->log_host;
+    h->log_host = nullptr;
+    return MHD_OK;
+  }
+  cudaMemPool_t pool;
+  rc = device_pool(h->device, &pool);
+  if (rc) return rc;
+  const size_t ring = (sizeof(LogEntry) * (size_t)capacity + 255) / 256 * 256;
+  const size_t part = sizeof(double) * 10 * DIAG_MAX_BLOCKS + 256;  // partials, then the ticket
+  CK(cudaMallocFromPoolAsync(&h->log_block, ring + part, pool, h->stream));
+  CK(cudaMemsetAsync(h->log_block, 0, ring + part, h->stream));
+  rc = read_ctrl(h);  // also orders the set-up before the caller's next use
+  if (rc) return rc;
+  h->log = static_cast<LogEntry*>(h->log_block);
+  h->diag_part = reinterpret_cast<double*>(static_cast<char*>(h->log_block) + ring);
+  h->log_cap = capacity;
+  h->diag = diagnostics != 0;
+  if (!h->log_host) h->log_host = new (std::nothrow) std::vector<LogEntry>();
+  if (!h->log_host) return MHD_ERR_INVALID;
+  h->log_host->clear();
+  h->log_host_seq = h->ctrl_host->log_seq;  // records of the past are not in this ring
+  h->log_dropped = 0;
+  return MHD_OK;
+}
+
+int mhd_gpu_read_log(mhd_gpu_t* h, mhd_log_entry* out, int cap, int* n, long long* dropped) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!n || cap < 0 || (cap > 0 && !out)) return MHD_ERR_INVALID;
+  if (!h->log) return MHD_ERR_STATE;
+  rc = read_ctrl(h);
+  if (rc) return rc;
+  rc = drain_log(h);
+  if (rc) return rc;
+  std::vector<LogEntry>& v = *h->log_host;
+  if (dropped) *dropped = h->log_dropped;
+  if (!out) {  // count only
+    *n = (int)std::min<size_t>(v.size(), 0x7fffffff);
+    return MHD_OK;
+  }
+  const size_t k = std::min<size_t>(v.size(), (size_t)cap);
+  std::memcpy(out, v.data(), sizeof(LogEntry) * k);
+  v.erase(v.begin(), v.begin() + (long)k);
+  *n = (int)k;
   return MHD_OK;
 }
 

@@ -331,7 +331,9 @@ __device__ __forceinline__ void ctl_stage_end_body(Ctrl* c) {
 
 // end of a try: accept (drive.f90:304-312) or prepare the re-try.  dt_lim is the value of the
 // last residual that ran, as in the reference, where every DG_semidiscretize overwrites it.
-__device__ __forceinline__ void ctl_step_end_body(Ctrl* c, int R) {
+// An accepted step appends its record to the log (drive.f90:314 log_append(t, tot_ent)); the
+// stage diagnostics of its final stage, which is the accepted state, are carried over.
+__device__ __forceinline__ void ctl_step_end_body(Ctrl* c, int R, LogEntry* log = nullptr, int log_cap = 0) {
   if (c->pending_dtlim) {
     c->dt_lim = dec_dtlim(c->dt_lim_bits);
     c->pending_dtlim = 0;
@@ -343,13 +345,68 @@ __device__ __forceinline__ void ctl_step_end_body(Ctrl* c, int R) {
   if (c->state != ST_RUN) return;
   c->t = c->t_rk[R];
   c->steps += 1;
+  const LogEntry* last = (log && log_cap > 0 && c->log_seq > 0) ? log + ((c->log_seq - 1) % log_cap) : nullptr;
+  if (LogEntry* e = log_next(log, log_cap, c)) {
+    e->step = c->steps;
+    e->kind = LOG_STEP;
+    e->stage = R;
+    e->try_num = c->try_num;
+    e->num_negcell = 0;
+    e->neg_avg = 0;
+    e->flags = c->flags;
+    e->t = c->t;
+    e->dt = c->dt;
+    e->dt_lim = c->dt_lim;
+    e->tot_ent = c->tot_ent;
+    if (last && last->kind == LOG_STAGE && last->step == c->steps && last->stage == R) {
+      e->rho_min = last->rho_min;
+      e->p_min = last->p_min;
+      for (int v = 0; v < 8; ++v) e->total[v] = last->total[v];
+    }
+  }
   c->try_num = 0;
   if (c->last_step) c->done = 1;
   c->state = ST_IDLE;
 }
 
+// The record of a stage that reached its end (drive.f90:285-294): the PP-limited cell count, or
+// the inadmissible average that abandons the try.  Called right after ctl_stage_end_body by the
+// thread that ran it, for a stage that was running when its end was reached.
+__device__ __forceinline__ void ctl_log_stage(Ctrl* c, int stage, LogEntry* log, int log_cap) {
+  LogEntry* e = log_next(log, log_cap, c);
+  if (!e) return;
+  e->step = c->steps + 1;
+  e->kind = LOG_STAGE;
+  e->stage = stage;
+  e->try_num = c->try_num;
+  e->neg_avg = c->neg_avg;
+  e->num_negcell = c->neg_avg ? 0 : c->num_negcell;
+  e->flags = c->flags;
+  e->t = c->t_rk[stage];
+  e->dt = c->dt;
+  e->dt_lim = __longlong_as_double(0x7ff8000000000000LL);
+  e->tot_ent = c->tot_ent;
+}
+
+// the record of the initial state (drive.f90:74 log_append(0, tot_ent)), written by solve_begin
+__global__ void ctl_log_initial(Ctrl* c, LogEntry* log, int log_cap) {
+  LogEntry* e = log_next(log, log_cap, c);
+  if (!e) return;
+  e->step = 0;
+  e->kind = LOG_STEP;
+  e->stage = 0;
+  e->try_num = 0;
+  e->num_negcell = 0;
+  e->neg_avg = 0;
+  e->flags = c->flags;
+  e->t = c->t;
+  e->dt = 0.0;
+  e->dt_lim = c->dt_lim;
+  e->tot_ent = c->tot_ent;
+}
+
 __global__ void ctl_step_begin(Ctrl* c) { ctl_step_begin_body(c); }
-__global__ void ctl_step_end(Ctrl* c, int R) { ctl_step_end_body(c, R); }
+__global__ void ctl_step_end(Ctrl* c, int R, LogEntry* log, int log_cap) { ctl_step_end_body(c, R, log, log_cap); }
 // the dt of the try and the pseudo-time of its first stage, in one launch
 __global__ void ctl_dt_stage1(Ctrl* c, int R) {
   ctl_dt_body(c);
@@ -391,7 +448,7 @@ __global__ void ctl_batched(const InstDesc* __restrict__ insts, const int* __res
         ctl_dt_body(c);
         ctl_stage_time_body(c, R, 1);
         break;
-      default: ctl_step_end_body(c, R); break;
+      default: ctl_step_end_body(c, R, insts[i].log, insts[i].log_cap); break;
     }
   }
 }

@@ -962,10 +962,12 @@ __device__ __forceinline__ void pp_entsum_body(const double* __restrict__ partia
 // stage was still running when the launch began.  A block that already sees the stage abandoned
 // skips its fill, and a fill of an abandoned stage only writes scratch ghosts, so the result is
 // that of the separate launches in sequence.
+// The stage's record goes to the driver log (log may be nullptr).
 template <int P>
 __global__ void __launch_bounds__(256) stage_end_bc_kernel(double* __restrict__ u, Geo g, Ctrl* ctrl, int R,
-                                                          int next_stage, const double* __restrict__ ent_partial,
-                                                          int ent_nblk) {
+                                                          int stage, int next_stage,
+                                                          const double* __restrict__ ent_partial, int ent_nblk,
+                                                          LogEntry* log, int log_cap) {
   __shared__ int s_run, s_ent;
   bool run;
   if (blockIdx.x == 0) {  // one read of the state for the whole block, before thread 0 updates it
@@ -978,6 +980,7 @@ __global__ void __launch_bounds__(256) stage_end_bc_kernel(double* __restrict__ 
     if (s_ent) pp_entsum_body(ent_partial, ent_nblk, ctrl);  // whole block
     if (threadIdx.x == 0) {
       ctl_stage_end_body(ctrl);
+      if (run) ctl_log_stage(ctrl, stage, log, log_cap);
       if (next_stage > 0) ctl_stage_time_body(ctrl, R, next_stage);
     }
   } else {
@@ -1021,9 +1024,84 @@ __global__ void __launch_bounds__(256) stage_end_bc_batched(const InstDesc* __re
     if (s_ent) pp_entsum_body(d.ent_partial, d.nseg_limit, d.ctrl);  // whole block
     if (threadIdx.x == 0) {
       ctl_stage_end_body(d.ctrl);
+      if (s_run) ctl_log_stage(d.ctrl, slot, d.log, d.log_cap);
       if (next_stage > 0) ctl_stage_time_body(d.ctrl, R, next_stage);
     }
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Stage diagnostics (optional, for checking the invariants the method promises): over the interior
+// nodes of a state, the minimum density, the minimum pressure (_macro_prs_, DG_solver.f90:125) and
+// the domain integrals of the eight conserved variables by the GLL rule the cell averages use
+// (sum of (hx hy / 4) w_k w_l u, DG_solver.f90:177-184,227-229).  Block b takes a fixed contiguous
+// range of elements and reduces in a fixed order; the last block to finish (a ticket counter, no
+// waiting) combines the block partials in block order and writes the newest log record.  The
+// result is therefore independent of timing.  `part` holds DIAG_MAX_BLOCKS x 10 doubles and the
+// ticket; the ticket is left at zero.
+// ---------------------------------------------------------------------------------------------
+constexpr int DIAG_MAX_BLOCKS = 592;  // 4 x 148 SMs
+
+template <int P>
+__global__ void __launch_bounds__(256) stage_diag_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
+                                                        double* __restrict__ part, unsigned int* ticket,
+                                                        LogEntry* log, int log_cap) {
+  constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
+  __shared__ double s[10][256];
+  __shared__ bool s_last;
+  if (!gate_open(ctrl, gate) || !log || log_cap <= 0 || ctrl->log_seq <= 0) return;
+  const int tid = threadIdx.x;
+  const int nx = g.nx, ny = g.ny;
+  const long long E = (long long)nx * ny;
+  const long long e0 = E * blockIdx.x / gridDim.x, e1 = E * (blockIdx.x + 1) / gridDim.x;
+  const DegConst& dc = c_deg[P];
+  const double gamma = g.gamma, q4 = 0.25 * g.hx * g.hy;
+  double rmin = 1.0e308, pmin = 1.0e308, acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long it = e0 * NN + tid; it < e1 * NN; it += 256) {
+    const long long e = it / NN;
+    const int q = (int)(it - e * NN), k = q % N, l = q / N;
+    const int j = 1 + (int)(e / nx), i = 1 + (int)(e - (long long)(j - 1) * nx);
+    const double* x = u + ((long long)j * (nx + 2) + i) * EB + q;
+    double w[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) w[v] = x[v * NN];
+    rmin = fmin(rmin, w[0]);
+    pmin = fmin(pmin, prs_of(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], gamma));
+    const double wq = q4 * dc.qw[k] * dc.qw[l];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) acc[v] += wq * w[v];
+  }
+  s[0][tid] = rmin;
+  s[1][tid] = pmin;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) s[2 + v][tid] = acc[v];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w) {
+      s[0][tid] = fmin(s[0][tid], s[0][tid + w]);
+      s[1][tid] = fmin(s[1][tid], s[1][tid + w]);
+#pragma unroll
+      for (int v = 2; v < 10; ++v) s[v][tid] = s[v][tid] + s[v][tid + w];
+    }
+    __syncthreads();
+  }
+  if (tid < 10) part[blockIdx.x * 10 + tid] = s[tid][0];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (tid < 10) {
+    const volatile double* vp = part;
+    double r = vp[tid];
+    for (unsigned b = 1; b < gridDim.x; ++b) r = tid < 2 ? fmin(r, vp[b * 10 + tid]) : r + vp[b * 10 + tid];
+    LogEntry* e = log + ((ctrl->log_seq - 1) % log_cap);
+    if (tid == 0) e->rho_min = r;
+    else if (tid == 1) e->p_min = r;
+    else e->total[tid - 2] = r;
+  }
+  if (tid == 0) *ticket = 0u;
 }
 
 }  // namespace mhd

@@ -59,7 +59,8 @@ def test_struct_layouts_match_the_header(pkg, tmp_path):
     import subprocess
     cap = pkg.capi
     structs = {"mhd_gpu_status": cap.Status, "mhd_request": cap.Request,
-               "mhd_request_result": cap.RequestResult, "mhd_server_stats": cap.ServerStats}
+               "mhd_request_result": cap.RequestResult, "mhd_server_stats": cap.ServerStats,
+               "mhd_log_entry": cap.LogEntry}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "mhd_gpu.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
@@ -80,6 +81,9 @@ def test_struct_layouts_match_the_header(pkg, tmp_path):
 
 def test_set_up_entry_points_reject_bad_arguments(pkg):
     lib = pkg.capi.load()
+    assert lib.mhd_gpu_set_log(None, 16, 0) == pkg.capi.MHD_ERR_INVALID
+    n = C.c_int()
+    assert lib.mhd_gpu_read_log(None, None, 0, C.byref(n), None) == pkg.capi.MHD_ERR_INVALID
     assert lib.mhd_gpu_init_problem(None, 0, None, 0) == pkg.capi.MHD_ERR_INVALID
     assert lib.mhd_gpu_download_avg_primitive(None, None, None, None) == pkg.capi.MHD_ERR_INVALID
 
