@@ -37,6 +37,9 @@ typedef struct mhd_gpu mhd_gpu_t;
 #define MHD_FLAG_PP_RELIMIT 2     /* PP re-limit failed (DG_solver.f90:582-586, error stop)  */
 #define MHD_FLAG_DT_COLLAPSE 4    /* dt collapse / too many retries (drive.f90:97-100)       */
 #define MHD_FLAG_INIT_NEG_AVG 8   /* initial value inadmissible (drive.f90:70)               */
+#define MHD_FLAG_DEVICE_WAIT 16   /* a kernel's bounded wait for its own asynchronous tile copy
+                                     ran out; the affected results are invalid (no reference
+                                     counterpart; not expected in normal operation)          */
 #define MHD_ERR_INVALID -1        /* bad argument                                            */
 #define MHD_ERR_UNSUPPORTED -2    /* configuration not supported by the kernels              */
 #define MHD_ERR_CUDA -3           /* a CUDA runtime call failed                              */

@@ -54,7 +54,7 @@ def ldf_operator(p, hx, hy):
 
 def _check(fn, rc, fatal_flags=True):
     if rc < 0 or (fatal_flags and rc & (capi.MHD_FLAG_PP_RELIMIT | capi.MHD_FLAG_DT_COLLAPSE |
-                                        capi.MHD_FLAG_INIT_NEG_AVG)):
+                                        capi.MHD_FLAG_INIT_NEG_AVG | capi.MHD_FLAG_DEVICE_WAIT)):
         raise MHDError(fn, rc)
     return rc
 

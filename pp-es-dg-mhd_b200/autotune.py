@@ -3,10 +3,11 @@
     python pp-es-dg-mhd_b200/autotune.py [--out PATH] [--jobs J]
 
 Builds the library once per candidate set (every set gives each degree p = 1, 2, 3 one tile
-configuration TX, TY, threads, CTAs per SM, face warps -- the MHD_RES_CFG<p> macros of
-csrc/residual.cuh), times the residual of each degree on a large mesh with CUDA events (each set
-in its own process), and writes the fastest configuration per degree as a header
-(csrc/residual_tuned.h by default), which the next build picks up.  Candidates whose tile does not
+configuration TX, TY, threads, CTAs per SM -- the MHD_RES2_CFG<p> macros of csrc/residual.cuh; a
+tile holds at most (threads / 32) * (32 / (p+1)^2) elements, one lane per node), times the residual
+of each degree on a large mesh with CUDA events (each set in its own process), and writes the
+fastest configuration per degree as a header (csrc/residual2_tuned.h by default), which the next
+build picks up.  Candidates whose tile does not
 fit one CTA's shared memory fail to compile and are skipped.  Needs a GPU for the timing.
 """
 import argparse
@@ -21,11 +22,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import build as B  # noqa: E402
 
-# (TX, TY, NT, MINB, HW) per degree; set i takes candidate i of every degree
+# (TX, TY, NT, MINB) per degree; set i takes candidate i of every degree
 CANDIDATES = {
-    1: [(4, 8, 128, 4, 3), (8, 4, 128, 4, 3), (8, 8, 256, 2, 5), (16, 4, 256, 2, 5)],
-    2: [(8, 4, 256, 2, 5), (4, 4, 128, 4, 3), (8, 4, 256, 2, 4), (4, 8, 256, 2, 5)],
-    3: [(4, 4, 256, 2, 5), (2, 4, 128, 4, 3), (4, 4, 256, 2, 6), (4, 2, 128, 4, 3)],
+    1: [(8, 8, 256, 2), (8, 4, 128, 4), (8, 6, 192, 3), (16, 4, 256, 2)],
+    2: [(6, 4, 256, 2), (4, 3, 128, 4), (6, 3, 192, 3), (8, 3, 256, 2)],
+    3: [(4, 4, 256, 2), (4, 2, 128, 4), (4, 3, 192, 3), (8, 2, 256, 2)],
 }
 MESHES = {1: 724, 2: 512, 3: 512}  # vortex, about 33 M DOFs each
 
@@ -34,7 +35,7 @@ def build_set(i, tmp):
     hdr = os.path.join(tmp, f"cfg{i}.h")
     with open(hdr, "w") as f:
         for p, cands in CANDIDATES.items():
-            f.write(f"#define MHD_RES_CFG{p} {', '.join(map(str, cands[i]))}\n")
+            f.write(f"#define MHD_RES2_CFG{p} {', '.join(map(str, cands[i]))}\n")
     objs = []
     try:
         for src in B.SOURCES:
@@ -85,7 +86,7 @@ print(json.dumps(out))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(B.CSRC, "residual_tuned.h"))
+    ap.add_argument("--out", default=os.path.join(B.CSRC, "residual2_tuned.h"))
     ap.add_argument("--jobs", type=int, default=4)
     args = ap.parse_args()
     nsets = len(CANDIDATES[1])
@@ -106,13 +107,13 @@ def main():
             print(f"set {i}: {times[i]}", flush=True)
     if not times:
         sys.exit("no candidate set could be timed")
-    lines = ["// residual_tuned.h -- written by autotune.py: residual tile per degree, fastest of the",
+    lines = ["// residual2_tuned.h -- written by autotune.py: residual tile per degree, fastest of the",
              "// candidates timed on this GPU (residual ms per launch, vortex mesh of about 33 M DOFs)."]
     for p in (1, 2, 3):
         best = min(times, key=lambda i: times[i][p])
         for i in sorted(times):
             lines.append(f"//   p={p} {CANDIDATES[p][i]}: {times[i][p]:.4f} ms{'  <- chosen' if i == best else ''}")
-        lines += [f"#ifndef MHD_RES_CFG{p}", f"#define MHD_RES_CFG{p} {', '.join(map(str, CANDIDATES[p][best]))}",
+        lines += [f"#ifndef MHD_RES2_CFG{p}", f"#define MHD_RES2_CFG{p} {', '.join(map(str, CANDIDATES[p][best]))}",
                   "#endif"]
     with open(args.out, "w") as f:
         f.write("\n".join(lines) + "\n")

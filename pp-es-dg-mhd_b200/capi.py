@@ -14,6 +14,7 @@ MHD_FLAG_NEG_AVG = 1
 MHD_FLAG_PP_RELIMIT = 2
 MHD_FLAG_DT_COLLAPSE = 4
 MHD_FLAG_INIT_NEG_AVG = 8
+MHD_FLAG_DEVICE_WAIT = 16
 
 IC_OT2PI, IC_OT_UNIT, IC_VORTEX, IC_BLAST, IC_ROTOR, IC_ALFVEN, IC_CLOUD_SHOCK, IC_JET = range(8)
 MHD_ERR_INVALID = -1

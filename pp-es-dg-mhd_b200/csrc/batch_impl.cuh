@@ -95,7 +95,7 @@ InstDesc make_desc(const mhd_gpu* h) {
 // items of each kind one member contributes (the same decomposition as its single-instance launches)
 template <int P>
 void member_work(const mhd_gpu* h, long long* cnt, InstDesc& d) {
-  using RL = ResLayout<P>;
+  using RL = Res2Layout<P>;
   constexpr int EB = 8 * (P + 1) * (P + 1), TE = PPCfg<P>::TE;
   const long long nx = h->nx, ny = h->ny;
   cnt[WK_RES] = ((nx + RL::TX - 1) / RL::TX) * ((ny + RL::TY - 1) / RL::TY);
@@ -198,7 +198,7 @@ template <int P>
 BatchGrids batch_grids(int nsm) {
   constexpr int EB = 8 * (P + 1) * (P + 1);
   BatchGrids gr;
-  gr.res = full_grid(residual_batched<P>, ResCfg<P>::NT, ResLayout<P>::BYTES, nsm);
+  gr.res = full_grid(residual2_batched<P>, Res2Layout<P>::NT, Res2Layout<P>::BYTES, nsm);
   gr.cmb = full_grid(combine_batched<EB>, 256, 0, nsm);
   gr.bc = full_grid(bc_batched<P>, 256, 0, nsm);
   gr.avg = full_grid(pp_avg_ldf_batched<P, false>, PP_NT, 0, nsm);
@@ -216,12 +216,13 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
   const int* tot = g.total();
   const int* ninst = g.ninst();
   InstDesc* in = g.insts();
-  const size_t smem = ResLayout<P>::BYTES;
+  const size_t smem = Res2Layout<P>::BYTES;
+  constexpr int NT_RES = Res2Layout<P>::NT;
   const int grid_res = gr.res, grid_cmb = gr.cmb, grid_bc = gr.bc, grid_avg = gr.avg, grid_sig = gr.sig,
             grid_lim = gr.lim;
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_BEGIN, R, 0);
-  residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE,
-                                                              0, 0.0, 0.0);
+  residual2_batched<P><<<grid_res, NT_RES, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE,
+                                                        0, 0.0, 0.0);
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_DT_STAGE1, R, 1);  // dt, and the pseudo-time of stage 1
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
@@ -248,8 +249,8 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
     const int nxt = (!fin && (R == 2 || R == 3)) ? s + 1 : 0;
     const double ca = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.75 : 1.0 / 3.0));
     const double cb = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.25 : 2.0 / 3.0));
-    residual_batched<P><<<grid_res, ResCfg<P>::NT, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, s, (s % R) + 1,
-                                                                ST_RUN, nxt, ca, cb);
+    residual2_batched<P><<<grid_res, NT_RES, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, s, (s % R) + 1,
+                                                          ST_RUN, nxt, ca, cb);
   }
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_END, R, 0);
 }
@@ -356,7 +357,7 @@ int batch_wait(mhd_batch* b, int* n_active) {
   if (n_active) {
     int a = 0;
     for (mhd_gpu* h : b->members)
-      if (!h->ctrl_host->done && !(h->ctrl_host->flags & 0xE)) ++a;
+      if (!h->ctrl_host->done && !(h->ctrl_host->flags & FLAGS_FATAL)) ++a;
     *n_active = a;
   }
   return MHD_OK;

@@ -31,6 +31,11 @@ struct DegConst {
 // Defined here: the device code of the library is one translation unit (mhd_gpu.cu).
 __constant__ DegConst c_deg[MAXP + 1];
 
+// Status flag bits of the control block (the MHD_FLAG_* values of mhd_gpu.h).  FLAGS_FATAL: the
+// bits that end a run (every bit but the per-stage inadmissible average).
+constexpr int FLAG_DEVICE_WAIT = 16;
+constexpr int FLAGS_FATAL = 2 | 4 | 8 | FLAG_DEVICE_WAIT;
+
 // Gate values: a kernel launched with gate >= 0 runs only if ctrl->state == gate.
 enum GateState : int { GATE_ALWAYS = -1, ST_IDLE = 0, ST_RUN = 1, ST_RECOMPUTE = 2, ST_FAILED = 3 };
 
@@ -190,6 +195,45 @@ inline double ord_dec_host(unsigned long long e) {
 
 __device__ __forceinline__ bool gate_open(const Ctrl* c, int gate) {
   return gate < 0 || c->state == gate;
+}
+
+// ---- asynchronous bulk copies global -> shared (sm_90+ cp.async.bulk, completed on an mbarrier) ---
+// Used for tile rows, which are contiguous runs of 16-byte aligned element blocks.  The source is
+// always this GPU's own memory; no multicast.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// one arrival that also announces `bytes` of copies completing on the barrier's current phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// `bytes` (a multiple of 16; both addresses 16-byte aligned) from global src to shared dst
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// orders this thread's earlier generic-proxy accesses of shared memory before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of `parity` to complete, at most `limit` polls (each poll may itself suspend
+// the thread for a short time).  Returns false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int limit = 1 << 22) {
+  for (int i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
 }
 
 // ---- physics (MHD_PDE.f90 formulas as inlined in DG_solver.f90) -------------------------------

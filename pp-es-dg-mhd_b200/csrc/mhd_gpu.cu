@@ -166,15 +166,15 @@ int init_device_tables(int dev) {
       }
   }
   CK(cudaMemcpyToSymbol(c_deg, tabs, sizeof(tabs)));
-  CK(cudaFuncSetAttribute(residual_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
-  CK(cudaFuncSetAttribute(residual_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
-  CK(cudaFuncSetAttribute(residual_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
-  CK(cudaFuncSetAttribute(residual_batched<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
-  CK(cudaFuncSetAttribute(residual_batched<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
-  CK(cudaFuncSetAttribute(residual_batched<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
-  CK(cudaFuncSetAttribute(residual_persistent<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<1>::BYTES));
-  CK(cudaFuncSetAttribute(residual_persistent<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<2>::BYTES));
-  CK(cudaFuncSetAttribute(residual_persistent<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ResLayout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_batched<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_batched<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_batched<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_persistent<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_persistent<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_persistent<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<3>::BYTES));
   g_dev_init[dev] = true;
   return MHD_OK;
 }
@@ -218,9 +218,9 @@ void launch_bc(mhd_gpu* h, double* u, int gate) {
 
 template <int P>
 void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate, StageCombine sc = StageCombine{}) {
-  using L = ResLayout<P>;
+  using L = Res2Layout<P>;
   dim3 grid((h->nx + L::TX - 1) / L::TX, (h->ny + L::TY - 1) / L::TY);
-  residual_kernel<P><<<grid, ResCfg<P>::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate, sc);
+  residual2_kernel<P><<<grid, L::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate, sc);
 }
 
 // the re-try residual of a try (gate ST_RECOMPUTE, usually closed): a persistent grid of the CTAs
@@ -232,17 +232,17 @@ int res_resident_ctas(int dev) {
   if (!cached[dev]) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, residual_persistent<P>, ResCfg<P>::NT,
-                                                  ResLayout<P>::BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, residual2_persistent<P>, Res2Layout<P>::NT,
+                                                  Res2Layout<P>::BYTES);
     cached[dev] = std::max(1, nsm) * std::max(1, per_sm);
   }
   return cached[dev];
 }
 template <int P>
 void launch_residual_retry(mhd_gpu* h, const double* u, double* ut) {
-  using L = ResLayout<P>;
+  using L = Res2Layout<P>;
   const int ntx = (h->nx + L::TX - 1) / L::TX, ntiles = ntx * ((h->ny + L::TY - 1) / L::TY);
-  residual_persistent<P><<<std::min(ntiles, res_resident_ctas<P>(h->device)), ResCfg<P>::NT, L::BYTES, h->stream>>>(
+  residual2_persistent<P><<<std::min(ntiles, res_resident_ctas<P>(h->device)), L::NT, L::BYTES, h->stream>>>(
       u, ut, h->geo, h->ctrl, ST_RECOMPUTE, ntx, ntiles);
 }
 
@@ -471,6 +471,7 @@ const char* mhd_gpu_status_string(int code) {
     case MHD_FLAG_PP_RELIMIT: return "positivity re-limit failed";
     case MHD_FLAG_DT_COLLAPSE: return "time step collapsed (too many re-tries or dt_lim < 1e-14)";
     case MHD_FLAG_INIT_NEG_AVG: return "initial value has an inadmissible cell average";
+    case MHD_FLAG_DEVICE_WAIT: return "a kernel's wait for its asynchronous copy ran out";
     case MHD_ERR_INVALID: return "invalid argument";
     case MHD_ERR_UNSUPPORTED: return "unsupported configuration";
     case MHD_ERR_CUDA: return "CUDA runtime error";
@@ -1045,7 +1046,7 @@ int mhd_gpu_state_device_ptr(mhd_gpu_t* h, int slot, double** dptr) {
 
 // =============================================================================================
 // Allocation-free residual.  Its only scratch (the dt_lim reduction cell and the status words of
-// the control block that residual_kernel writes) lives in this file-scope static device array;
+// the control block that the residual kernel writes) lives in this file-scope static device array;
 // host code reaches it through the address cudaGetSymbolAddress returns for the current device.
 // =============================================================================================
 namespace {
@@ -1107,18 +1108,18 @@ extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, 
   g.gamma = gamma;
   switch (p) {
     case 1: {
-      using L = ResLayout<1>;
-      residual_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<1>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
+      using L = Res2Layout<1>;
+      residual2_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     case 2: {
-      using L = ResLayout<2>;
-      residual_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<2>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
+      using L = Res2Layout<2>;
+      residual2_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     default: {
-      using L = ResLayout<3>;
-      residual_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), ResCfg<3>::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
+      using L = Res2Layout<3>;
+      residual2_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
   }

@@ -232,7 +232,7 @@ __device__ __forceinline__ void ctl_step_begin_body(Ctrl* c) {
     c->dt_lim = dec_dtlim(c->dt_lim_bits);
     c->pending_dtlim = 0;
   }
-  if (c->done || (c->flags & 0xE) || c->steps >= c->step_limit) {  // finished, error, or step budget used
+  if (c->done || (c->flags & FLAGS_FATAL) || c->steps >= c->step_limit) {  // finished, error, or step budget used
     c->state = ST_IDLE;
     return;
   }

@@ -218,7 +218,7 @@ int retire_finished(mhd_server* s) {
   const auto t0 = std::chrono::steady_clock::now();
   for (size_t k = 0; k < s->active.size();) {
     const Ctrl* c = s->active[k].h->ctrl_host;
-    if (c->done || (c->flags & 0xE)) {
+    if (c->done || (c->flags & FLAGS_FATAL)) {
       int rc = retire(s, k);
       if (rc) return rc;
     } else {

@@ -20,6 +20,7 @@ module mhd_gpu_bind
   integer(c_int), parameter :: MHD_OK = 0
   integer(c_int), parameter :: MHD_FLAG_NEG_AVG = 1, MHD_FLAG_PP_RELIMIT = 2
   integer(c_int), parameter :: MHD_FLAG_DT_COLLAPSE = 4, MHD_FLAG_INIT_NEG_AVG = 8
+  integer(c_int), parameter :: MHD_FLAG_DEVICE_WAIT = 16
   integer(c_int), parameter :: MHD_ERR_INVALID = -1, MHD_ERR_UNSUPPORTED = -2, MHD_ERR_CUDA = -3
   integer(c_int), parameter :: MHD_ERR_NO_DEVICE = -4, MHD_ERR_STATE = -5
   ! boundary-condition kinds (replace the BC_handle procedure pointer, drive.f90:25)

@@ -103,20 +103,22 @@ def test_autotune_candidates_are_well_formed():
     sets = {len(c) for c in at.CANDIDATES.values()}
     assert len(sets) == 1  # set i takes candidate i of every degree
     for p, cands in at.CANDIDATES.items():
-        for tx, ty, nt, minb, hw in cands:
-            assert nt % 32 == 0 and nt <= 512 and 1 <= hw <= nt // 32 and tx >= 1 and ty >= 1 and minb >= 1
+        for tx, ty, nt, minb in cands:
+            # one lane per node: a warp holds 32 // (p+1)^2 elements
+            assert nt % 32 == 0 and nt <= 1024 and tx >= 1 and ty >= 1 and minb >= 1
+            assert tx * ty <= (nt // 32) * (32 // (p + 1) ** 2)
 
 
 def test_tuned_header_defines_every_degree():
-    path = os.path.join(ROOT, "pp-es-dg-mhd_b200", "csrc", "residual_tuned.h")
+    path = os.path.join(ROOT, "pp-es-dg-mhd_b200", "csrc", "residual2_tuned.h")
     if not os.path.exists(path):
         return
     text = open(path).read()
     for p in (1, 2, 3):
-        m = re.search(rf"#define MHD_RES_CFG{p} (\d+), (\d+), (\d+), (\d+), (\d+)", text)
+        m = re.search(rf"#define MHD_RES2_CFG{p} (\d+), (\d+), (\d+), (\d+)", text)
         assert m, p
-        tx, ty, nt, minb, hw = map(int, m.groups())
-        assert nt % 32 == 0 and 1 <= hw <= nt // 32
+        tx, ty, nt, minb = map(int, m.groups())
+        assert nt % 32 == 0 and tx * ty <= (nt // 32) * (32 // (p + 1) ** 2)
 
 
 def test_noalloc_rejects_misaligned_and_overlapping_buffers_on_the_host(pkg):
