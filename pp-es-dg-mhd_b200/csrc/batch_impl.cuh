@@ -201,10 +201,10 @@ BatchGrids batch_grids(int nsm) {
   gr.res = full_grid(residual2_batched<P>, Res2Layout<P>::NT, Res2Layout<P>::BYTES, nsm);
   gr.cmb = full_grid(combine_batched<EB>, 256, 0, nsm);
   gr.bc = full_grid(bc_batched<P>, 256, 0, nsm);
-  gr.avg = full_grid(pp_avg_ldf_batched<P, false>, PP_NT, 0, nsm);
-  gr.avg_final = full_grid(pp_avg_ldf_batched<P, true>, PP_NT, 0, nsm);
+  gr.avg = full_grid(pp_avg_ldf_batched<P, false>, PPCfg<P>::NT, 0, nsm);
+  gr.avg_final = full_grid(pp_avg_ldf_batched<P, true>, PPCfg<P>::NT, 0, nsm);
   gr.sig = full_grid(pp_sigsum_batched<P>, 256, 0, nsm);
-  gr.lim = full_grid(pp_limit_batched<P>, PP_NT, 0, nsm);
+  gr.lim = full_grid(pp_limit_batched<P>, PPCfg<P>::NT, 0, nsm);
   gr.seb = full_grid(stage_end_bc_batched<P>, 256, 0, nsm);
   return gr;
 }
@@ -232,16 +232,16 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
       combine_batched<EB><<<grid_cmb, 256, 0, st>>>(in, g.pref(WK_CMB), tot + WK_CMB, ninst, s, ST_RUN);
     if (s > 1) bc_batched<P><<<grid_bc, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, ST_RUN);
     if (fin)
-      pp_avg_ldf_batched<P, true><<<gr.avg_final, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN,
+      pp_avg_ldf_batched<P, true><<<gr.avg_final, PPCfg<P>::NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN,
                                                                   s == 1);
     else
-      pp_avg_ldf_batched<P, false><<<grid_avg, PP_NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN,
+      pp_avg_ldf_batched<P, false><<<grid_avg, PPCfg<P>::NT, 0, st>>>(in, g.pref(WK_AVG), tot + WK_AVG, ninst, s, ST_RUN,
                                                                 s == 1);
     if (fin) {
       pp_reduce_batched<<<b->nsm, 256, 0, st>>>(in, ninst, fin, ST_RUN);
       pp_sigsum_batched<P><<<grid_sig, 256, 0, st>>>(in, g.pref(WK_SIG), tot + WK_SIG, ninst, s, fin, ST_RUN);
     }
-    if (fin) pp_limit_batched<P><<<grid_lim, PP_NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
+    if (fin) pp_limit_batched<P><<<grid_lim, PPCfg<P>::NT, 0, st>>>(in, g.pref(WK_LIM), tot + WK_LIM, ninst, s, fin, ST_RUN);
     // entropy sum (final stage), stage-end decision, next stage's pseudo-time and the ghost rings
     stage_end_bc_batched<P><<<gr.seb, 256, 0, st>>>(in, g.pref(WK_BC), tot + WK_BC, ninst, s, R, fin ? 0 : s + 1,
                                                      fin);

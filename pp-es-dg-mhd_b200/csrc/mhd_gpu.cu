@@ -108,7 +108,7 @@ InstLayout inst_layout(int nx, int ny, int p, int R) {
   L.ldfA = take(sizeof(double) * n2 * n2);
   L.sig_x = take(sizeof(double) * 8 * (size_t)(nx + 1) * ny);
   L.sig_y = take(sizeof(double) * 8 * (size_t)nx * (ny + 1));
-  const size_t te_min = 16;  // the smallest elements-per-CTA of the post-process kernels
+  const size_t te_min = pp_min_chunk();  // the smallest elements-per-CTA of the post-process kernels
   L.partial = take(sizeof(double) * 8 * ((nelg + te_min - 1) / te_min + 1));
   L.ent_partial = take(sizeof(double) * (((size_t)nx + te_min - 1) / te_min + 1) * ny);
   L.cell_ent_DG = take(sizeof(double) * nelg);
@@ -136,7 +136,7 @@ int pp_resident_ctas(int dev) {
   if (!cached[dev]) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pp_avg_ldf_kernel<P, NEEDG>, PP_NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pp_avg_ldf_kernel<P, NEEDG>, PPCfg<P>::NT, 0);
     cached[dev] = std::max(1, nsm) * std::max(1, per_sm);
   }
   return cached[dev];
@@ -270,12 +270,12 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
   const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
   if (apply_oedg) {
     const int grid1 = std::min(nb1, pp_resident_ctas<P, true>(h->device));
-    pp_avg_ldf_kernel<P, true><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
+    pp_avg_ldf_kernel<P, true><<<grid1, PPCfg<P>::NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
                                                                 1, ent_offset, h->partial, h->cell_ent_DG,
                                                                 h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1, s1);
   } else {
     const int grid1 = std::min(nb1, pp_resident_ctas<P, false>(h->device));
-    pp_avg_ldf_kernel<P, false><<<grid1, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
+    pp_avg_ldf_kernel<P, false><<<grid1, PPCfg<P>::NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_ldf,
                                                                  0, ent_offset, h->partial, h->cell_ent_DG,
                                                                  h->cell_ent_FV, h->cell_ent_nan, limit_in_loop1, nb1, s1);
   }
@@ -290,7 +290,7 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
     cudaStreamWaitEvent(h->stream, h->ev_join, 0);
   }
   dim3 g3 = pp_grid_limit<P>(h);
-  pp_limit_kernel<P><<<g3, PP_NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_oedg, dt_ptr,
+  pp_limit_kernel<P><<<g3, PPCfg<P>::NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_oedg, dt_ptr,
                                                    oedg_dt, ent_offset, comput_ent, h->sig_x, h->sig_y,
                                                    h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan,
                                                    h->ent_partial, accept_dst);

@@ -24,7 +24,7 @@
 // of a variable are then 8*NN-byte runs per group (coalesced), per-element sums, minima and maxima
 // are butterfly reductions inside the group (every lane ends with the same value, since IEEE
 // addition, min and max are commutative), and no CTA-wide barrier sits between the steps of one
-// element.  A CTA of PP_NT threads handles a chunk of TE = (PP_NT/32) * (32/GS) consecutive
+// element.  A CTA of NT threads handles a chunk of TE = (NT/32) * (32/GS) consecutive
 // elements; per-chunk partial sums are formed in element order.  The single-instance loop-1
 // kernel is a persistent grid over the chunks in which each warp copies its elements of the next
 // chunk into shared memory (cp.async) while it works on the current one.  In the first stage of
@@ -36,17 +36,71 @@
 
 namespace mhd {
 
-constexpr int PP_NT = 256;
-constexpr int PP_MINB = 4;  // CTAs per SM the loop-1/loop-3 kernels are register-budgeted for
 constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// Per degree: threads per CTA and CTAs per SM (the register budget) of the loop-1 and loop-3
+// kernels (MHD_PP_CFG<p> = NT, MINB), and the element tile and CTAs per SM of the OEDG indicator
+// kernel (MHD_SIG_CFG<p> = TX, TY, MINB).  autotune.py times candidates on the GPU at hand and
+// writes post_tuned.h, which takes precedence when present.
+#if __has_include("post_tuned.h")
+#include "post_tuned.h"
+#endif
+#ifndef MHD_PP_CFG1
+#define MHD_PP_CFG1 256, 4
+#endif
+#ifndef MHD_PP_CFG2
+#define MHD_PP_CFG2 256, 4
+#endif
+#ifndef MHD_PP_CFG3
+#define MHD_PP_CFG3 256, 4
+#endif
+#ifndef MHD_SIG_CFG1
+#define MHD_SIG_CFG1 8, 8, 3
+#endif
+#ifndef MHD_SIG_CFG2
+#define MHD_SIG_CFG2 8, 4, 3
+#endif
+#ifndef MHD_SIG_CFG3
+#define MHD_SIG_CFG3 4, 4, 2
+#endif
+struct PPParams {
+  int NT, MINB;
+};
+struct SigParams {
+  int TX, TY, MINB;
+};
+template <int P>
+struct PPTune;
+template <>
+struct PPTune<1> {
+  static constexpr PPParams pp{MHD_PP_CFG1};
+  static constexpr SigParams sig{MHD_SIG_CFG1};
+};
+template <>
+struct PPTune<2> {
+  static constexpr PPParams pp{MHD_PP_CFG2};
+  static constexpr SigParams sig{MHD_SIG_CFG2};
+};
+template <>
+struct PPTune<3> {
+  static constexpr PPParams pp{MHD_PP_CFG3};
+  static constexpr SigParams sig{MHD_SIG_CFG3};
+};
 
 template <int P>
 struct PPCfg {
   static constexpr int N = P + 1, NN = N * N, EB = 8 * NN, N2 = 2 * NN;
+  static constexpr int NT = PPTune<P>::pp.NT, MINB = PPTune<P>::pp.MINB;
   static constexpr int GS = NN <= 4 ? 4 : (NN <= 8 ? 8 : (NN <= 16 ? 16 : 32));  // lanes per element
   static constexpr int G = 32 / GS;                                               // elements per warp
-  static constexpr int TE = (PP_NT / 32) * G;                                     // elements per CTA chunk
+  static constexpr int TE = (NT / 32) * G;                                        // elements per CTA chunk
+  static_assert(NT % 32 == 0 && NT <= 1024, "whole warps");
 };
+// the smallest chunk of any degree: per-chunk partial buffers are sized by it
+constexpr int pp_min_chunk() {
+  return PPCfg<1>::TE < PPCfg<2>::TE ? (PPCfg<1>::TE < PPCfg<3>::TE ? PPCfg<1>::TE : PPCfg<3>::TE)
+                                     : (PPCfg<2>::TE < PPCfg<3>::TE ? PPCfg<2>::TE : PPCfg<3>::TE);
+}
 
 // global -> shared copies that do not pass through registers (cp.async, sm_80 and later): 8 bytes,
 // or 16 bytes with both addresses 16-byte aligned
@@ -441,7 +495,7 @@ __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s
   constexpr int N2 = PPCfg<P>::N2;
   constexpr int NN = PPCfg<P>::NN;
   // pair (A[node][m], A[NN + node][m]) at m * NN + node; A is stored column-major (row + N2 * m)
-  for (int it = threadIdx.x; it < N2 * NN; it += PP_NT) {
+  for (int it = threadIdx.x; it < N2 * NN; it += PPCfg<P>::NT) {
     const int m = it / NN, node = it - m * NN;
     s_A[2 * it] = __ldg(A + node + N2 * m);
     s_A[2 * it + 1] = __ldg(A + NN + node + N2 * m);
@@ -451,7 +505,7 @@ __device__ __forceinline__ void load_ldf(const double* __restrict__ A, double* s
 // one CTA walks chunks blockIdx.x, blockIdx.x + gridDim.x, ... (the LDF operator is loaded once).
 // NEEDG: the OEDG form (need_global), with the per-chunk partial sums of the averages.
 template <int P, bool NEEDG>
-__global__ void __launch_bounds__(PP_NT, PP_MINB)
+__global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     pp_avg_ldf_kernel(double* __restrict__ u, double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                       int gate, int apply_ldf, int need_global, int ent_offset,
                       double* __restrict__ partial_sum,  // [chunks][8]
@@ -461,7 +515,7 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
   __shared__ __align__(16) double s_A[C::N2 * C::N2];
   __shared__ __align__(16) double s_ldf[C::TE * (C::N2 + 2)];
   __shared__ double s_red[2 * C::TE * 8];  // chunk sums, two buffers used in turn
-  __shared__ __align__(16) double s_pf[(PP_NT / 32) * 2 * C::G * C::EB];  // per warp: u (or u_con), k1
+  __shared__ __align__(16) double s_pf[(C::NT / 32) * 2 * C::G * C::EB];  // per warp: u (or u_con), k1
   __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
   if (threadIdx.x == 0) s_cnt = 0;
@@ -490,7 +544,7 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
 // final-stage form (OEDG global reductions for instances that use OEDG); the other stages fuse
 // loop 3 (limit)
 template <int P, bool FINAL>
-__global__ void __launch_bounds__(PP_NT, FINAL ? 3 : PP_MINB)
+__global__ void __launch_bounds__(PPCfg<P>::NT, FINAL ? (PPCfg<P>::MINB > 3 ? 3 : PPCfg<P>::MINB) : PPCfg<P>::MINB)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate,
                        int stage1) {
@@ -662,13 +716,9 @@ __device__ __forceinline__ double sigsum_coef(int n, int t, double h) {
 }
 
 template <int P>
-struct SigCfg;
-template <>
-struct SigCfg<1> { static constexpr int TX = 8, TY = 8; };
-template <>
-struct SigCfg<2> { static constexpr int TX = 8, TY = 4; };
-template <>
-struct SigCfg<3> { static constexpr int TX = 4, TY = 4; };
+struct SigCfg {
+  static constexpr int TX = PPTune<P>::sig.TX, TY = PPTune<P>::sig.TY, MINB = PPTune<P>::sig.MINB;
+};
 
 template <int P>
 struct SigLayout {
@@ -780,8 +830,7 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
 }
 
 template <int P>
-// 3 CTAs per SM where the face math fits 80 registers (p <= 2); p = 3 needs 2 (it spills at 80)
-__global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
+__global__ void __launch_bounds__(256, SigCfg<P>::MINB)
     pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
                      double* __restrict__ sig_x, double* __restrict__ sig_y) {
   if (!gate_open(ctrl, gate)) return;
@@ -790,7 +839,7 @@ __global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
 
 // many instances: items = every member's tiles (row-major)
 template <int P>
-__global__ void __launch_bounds__(256, P == 3 ? 2 : 3)
+__global__ void __launch_bounds__(256, SigCfg<P>::MINB)
     pp_sigsum_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   const int nw = *nwork, n = *ninst;
@@ -895,7 +944,7 @@ __device__ __forceinline__ void pp_limit_segment(
 }
 
 template <int P>
-__global__ void __launch_bounds__(PP_NT, PP_MINB)
+__global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     pp_limit_kernel(double* __restrict__ u, const double* __restrict__ u_avg, Geo g, Ctrl* ctrl,
                     int gate, int apply_oedg, const double* __restrict__ dt_ptr, double oedg_dt_arg,
                     int ent_offset, int comput_ent, const double* __restrict__ sig_x,
@@ -918,7 +967,7 @@ __global__ void __launch_bounds__(PP_NT, PP_MINB)
 // many instances: items = every member's row segments (row-major); the final stage applies OEDG
 // (if the instance uses it), computes the entropy and writes the accepted interior into slot 0
 template <int P>
-__global__ void __launch_bounds__(PP_NT, PP_MINB)
+__global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   __shared__ double s_ent[PPCfg<P>::TE];

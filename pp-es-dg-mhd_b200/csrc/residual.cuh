@@ -763,86 +763,22 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
     sgx = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
     sgy = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
   }
-  double acc[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) acc[v] = 0.0;
   auto Dm = [&](int i) { return s_dm[i]; };
-  // This lane's flux with the node in lane `src` (x frame, or y through swap_xy); the result F is
-  // in the global frame.  Every lane of the warp calls it (the shuffles need the full warp).
-  auto pair_flux = [&](int src, bool ydir, double* F) {
-    double A[8], B[8], Fx[8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) B[v] = __shfl_sync(FULL, pp[v], src);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      const int sv = swap_xy_var(v);
-      A[v] = ydir ? pp[sv] : pp[v];
-      const double b = ydir ? B[sv] : B[v];
-      Fx[v] = b;  // reuse as the rotated partner
-    }
-    ec_flux<0>(A, Fx, igm1, B);
-#pragma unroll
-    for (int v = 0; v < 8; ++v) F[v] = ydir ? B[swap_xy_var(v)] : B[v];
-  };
   // the partner lane of node (kk, ll) of this lane's element
   auto lane_of = [&](int kk, int ll) { return gbase + kk + N * ll; };
-  if constexpr (P == 1) {
-    const bool xb = (k == l);
-    double F[8];
-    pair_flux(xb ? lane_of(1 - k, l) : lane_of(k, 1 - l), !xb, F);
-    const double c1 = xb ? 2.0 * sxh * Dm(k + N * (1 - k)) : 2.0 * syh * Dm(l + N * (1 - l));
-#pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] -= c1 * F[v];
-    const int src2 = xb ? lane_of(k, 1 - l) : lane_of(1 - k, l);
-    const double c2 = xb ? 2.0 * syh * Dm(l + N * (1 - l)) : 2.0 * sxh * Dm(k + N * (1 - k));
-#pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] -= c2 * __shfl_sync(FULL, F[v], src2);
-  } else {
-    // rings along x and y: compute with the next node, receive from the previous one
-#pragma unroll
-    for (int dir = 0; dir < 2; ++dir) {
-      const int a = dir == 0 ? k : l;
-      const int an = (a + 1) % N, ap = (a + N - 1) % N;
-      const double h2 = dir == 0 ? 2.0 * sxh : 2.0 * syh;
-      double F[8];
-      pair_flux(dir == 0 ? lane_of(an, l) : lane_of(k, an), dir == 1, F);
-      const double c1 = h2 * Dm(a + N * an), c2 = h2 * Dm(a + N * ap);
-      const int src2 = dir == 0 ? lane_of(ap, l) : lane_of(k, ap);
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        if (v == (dir == 0 ? 4 : 5)) continue;  // that component of the flux is identically zero
-        acc[v] -= c1 * F[v];
-        acc[v] -= c2 * __shfl_sync(FULL, F[v], src2);
-      }
-    }
-    if constexpr (P == 3) {  // the pairs (k, k^2) along x and (l, l^2) along y
-      const bool xb = ((k >> 1) ^ (l >> 1)) == 0;
-      double F[8];
-      pair_flux(xb ? lane_of(k ^ 2, l) : lane_of(k, l ^ 2), !xb, F);
-      const double cx = 2.0 * sxh * Dm(k + N * (k ^ 2)), cy = 2.0 * syh * Dm(l + N * (l ^ 2));
-      const int src2 = xb ? lane_of(k, l ^ 2) : lane_of(k ^ 2, l);
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        acc[v] -= (xb ? cx : cy) * F[v];
-        acc[v] -= (xb ? cy : cx) * __shfl_sync(FULL, F[v], src2);
-      }
-    }
-  }
   // local div B (DG_solver.f90:813), the sums in node order
   double dbx = 0.0, dby = 0.0;
 #pragma unroll
   for (int r = 0; r < N; ++r) dbx += Dm(k + N * r) * __shfl_sync(FULL, w[4], lane_of(r, l));
 #pragma unroll
   for (int m = 0; m < N; ++m) dby += __shfl_sync(FULL, w[5], lane_of(k, m)) * Dm(l + N * m);
-
-  __syncthreads();  // the interface fluxes of phase 1 are complete
-
-  // ---- phase 3: node flux, diagonal, Godunov-Powell and surface terms; dt_lim; store ----
-  {
+  // node flux F, G and Godunov-Powell coefficients (DG_solver.f90:749-799), formed again for the
+  // surface terms after the barrier; the accumulation starts, as the reference's does
+  // (DG_solver.f90:833), with the diagonal and Godunov-Powell terms
+  auto node_fluxes = [&](double* F, double* Gf, double* GP) {
     const double bx = w[4], by = w[5], bz = w[6];
     const double bu = bx * vx + by * vy + bz * vz;
     const double ex = by * vz - bz * vy, ey = bz * vx - bx * vz, ez = bx * vy - by * vx;
-    double F[8], Gf[8], GP[8];
     F[0] = w[1];
     F[1] = vx * w[1] - bx * bx + pt;
     F[2] = vx * w[2] - by * bx;
@@ -867,10 +803,97 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
     GP[5] = vy;
     GP[6] = vz;
     GP[7] = bu;
+  };
+  double acc[8];
+  {
+    double F[8], Gf[8], GP[8];
+    node_fluxes(F, Gf, GP);
     const double divB = sxh * dbx + syh * dby;
     const double ckk = 2.0 * sxh * Dm(k + N * k), cll = 2.0 * syh * Dm(l + N * l);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] = acc[v] - ckk * F[v] - cll * Gf[v] - divB * GP[v];
+    for (int v = 0; v < 8; ++v) acc[v] = -(ckk * F[v]) - cll * Gf[v] - divB * GP[v];
+  }
+  // This lane's flux with the node in lane `src` (x frame, or y through swap_xy); the result F is
+  // in the global frame.  Every lane of the warp calls it (the shuffles need the full warp).
+  auto pair_flux = [&](int src, bool ydir, double* F) {
+    double A[8], B[8], Fx[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) B[v] = __shfl_sync(FULL, pp[v], src);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const int sv = swap_xy_var(v);
+      A[v] = ydir ? pp[sv] : pp[v];
+      const double b = ydir ? B[sv] : B[v];
+      Fx[v] = b;  // reuse as the rotated partner
+    }
+    ec_flux<0>(A, Fx, igm1, B);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) F[v] = ydir ? B[swap_xy_var(v)] : B[v];
+  };
+  if constexpr (P == 1) {
+    const bool xb = (k == l);
+    double F[8];
+    pair_flux(xb ? lane_of(1 - k, l) : lane_of(k, 1 - l), !xb, F);
+    const double c1 = xb ? 2.0 * sxh * Dm(k + N * (1 - k)) : 2.0 * syh * Dm(l + N * (1 - l));
+    const int src2 = xb ? lane_of(k, 1 - l) : lane_of(1 - k, l);
+    const double c2 = xb ? 2.0 * syh * Dm(l + N * (1 - l)) : 2.0 * sxh * Dm(k + N * (1 - k));
+    // the reference's order: x partner below, y partner below, x above, y above
+    const int rx = (1 - k) < k ? 0 : 2, ry = (1 - l) < l ? 1 : 3;
+    const bool own_first = xb ? rx < ry : ry < rx;
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const double fr = __shfl_sync(FULL, F[v], src2);
+      const double t1 = own_first ? c1 * F[v] : c2 * fr, t2 = own_first ? c2 * fr : c1 * F[v];
+      acc[v] -= t1;
+      acc[v] -= t2;
+    }
+  } else {
+    // rings along x and y: compute with the next node, receive from the previous one
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      const int a = dir == 0 ? k : l;
+      const int an = (a + 1) % N, ap = (a + N - 1) % N;
+      const double h2 = dir == 0 ? 2.0 * sxh : 2.0 * syh;
+      double F[8];
+      pair_flux(dir == 0 ? lane_of(an, l) : lane_of(k, an), dir == 1, F);
+      const double c1 = h2 * Dm(a + N * an), c2 = h2 * Dm(a + N * ap);
+      const int src2 = dir == 0 ? lane_of(ap, l) : lane_of(k, ap);
+      const bool next_first = an < ap;  // the two contributions in ascending partner order
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        if (v == (dir == 0 ? 4 : 5)) continue;  // that component of the flux is identically zero
+        const double fr = __shfl_sync(FULL, F[v], src2);
+        const double t1 = next_first ? c1 * F[v] : c2 * fr, t2 = next_first ? c2 * fr : c1 * F[v];
+        acc[v] -= t1;
+        acc[v] -= t2;
+      }
+    }
+    if constexpr (P == 3) {  // the pairs (k, k^2) along x and (l, l^2) along y
+      const bool xb = ((k >> 1) ^ (l >> 1)) == 0;
+      double F[8];
+      pair_flux(xb ? lane_of(k ^ 2, l) : lane_of(k, l ^ 2), !xb, F);
+      const double cx = 2.0 * sxh * Dm(k + N * (k ^ 2)), cy = 2.0 * syh * Dm(l + N * (l ^ 2));
+      const int src2 = xb ? lane_of(k, l ^ 2) : lane_of(k ^ 2, l);
+      // the reference's order: x partner below, y partner below, x above, y above
+      const int rx = (k ^ 2) < k ? 0 : 2, ry = (l ^ 2) < l ? 1 : 3;
+      const bool own_first = xb ? rx < ry : ry < rx;
+      const double c1 = xb ? cx : cy, c2 = xb ? cy : cx;
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        const double fr = __shfl_sync(FULL, F[v], src2);
+        const double t1 = own_first ? c1 * F[v] : c2 * fr, t2 = own_first ? c2 * fr : c1 * F[v];
+        acc[v] -= t1;
+        acc[v] -= t2;
+      }
+    }
+  }
+  __syncthreads();  // the interface fluxes of phase 1 are complete
+
+  // ---- phase 3: surface terms; dt_lim; store ----
+  {
+    const double bx = w[4], by = w[5];
+    double F[8], Gf[8], GP[8];
+    node_fluxes(F, Gf, GP);
     // surface terms (DG_solver.f90:872-882): left face (k = 0) with -, right face (k = N-1) with +;
     // likewise bottom/top in y
     if (k == 0 || k == N - 1) {

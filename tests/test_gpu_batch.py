@@ -158,3 +158,38 @@ def test_members_with_mixed_solve_flags_identical_to_solo_runs(pkg):
         for m, (u_ref, _) in zip(members, solo):
             np.testing.assert_array_equal(m.download_state(0), u_ref)
             m.close()
+
+
+@pytest.mark.parametrize("rknstg", [3, 2])
+def test_batch_members_against_the_oracle(pkg, ora, rknstg):
+    """each member of a mixed batch (degrees 1-3, different problems and meshes) against its own
+    oracle run: the batched kernels themselves (residual2_batched, pp_*_batched,
+    stage_end_bc_batched, ctl_batched) at the parity bar, not only through the solo path"""
+    from conftest import rel_l1
+    K = 4
+    specs = [("ot2pi", 14, 2, 1.0, None), ("rotor", 12, 1, 1.2, None), ("blast", 10, 3, 1.0, None)]
+    members, probs = [], []
+    with pkg.Batch() as b:
+        for name, n, p, amp, gamma in specs:
+            prob = pkg.problems.make(name, gamma=gamma, amp=amp)
+            s = pkg.DGSolver.for_problem(prob, n, n, p, rknstg)
+            s.upload_state(0, prob.initial_state(n, n, p))
+            s.solve_begin(prob.final_T, prob.cfl)
+            b.add(s)
+            members.append(s)
+            probs.append(prob)
+        b.advance(K)
+        sts = [b.status(s) for s in members]
+        for s in members:
+            b.remove(s)
+    for s, st, prob, (name, n, p, amp, gamma) in zip(members, sts, probs, specs):
+        o = ora.OracleSolver(n, n, p, p, rknstg, *prob.domain, prob.gamma, prob.bc_kind, prob.bc_state)
+        o.set_state(prob.initial_state(n, n, p)[:, :, :, 1:-1, 1:-1])
+        so = o.solve(prob.final_T, prob.cfl, max_steps=K)
+        assert st["steps"] == so["steps"] == K and st["retries"] == so["retries"]
+        err = rel_l1(s.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
+        assert err.max() <= 1e-12, (name, p, err)
+        assert abs(st["t"] - so["t"]) <= 1e-14 * so["t"]
+        assert st["num_negcell_total"] == so["num_negcell_total"]
+        o.close()
+        s.close()

@@ -1,7 +1,10 @@
 """Serving loop (GPU): continuous batching returns, for every request, exactly the solve a plain
-run gives; admission respects the HBM budget; the one-at-a-time mode serves the same queue."""
+run gives, and the solve the oracle gives at the parity bar; admission respects the HBM budget; the
+one-at-a-time mode serves the same queue."""
 import numpy as np
 import pytest
+
+from conftest import rel_l1
 
 pytestmark = pytest.mark.gpu
 
@@ -17,7 +20,7 @@ def _solo_avg(pkg, name, n, p, t_end):
 
 
 @pytest.mark.parametrize("batched", [True, False])
-def test_served_results_identical_to_plain_runs(pkg, batched):
+def test_served_results_identical_to_plain_runs(pkg, ora, batched):
     with pkg.Server(hbm_budget_bytes=8 << 30, tries_per_round=2, batched=batched) as srv:
         avgs = []
         for i, (name, n, p, arr, t_end) in enumerate(REQS):
@@ -35,6 +38,15 @@ def test_served_results_identical_to_plain_runs(pkg, batched):
             assert r["steps"] == st["steps"] and r["t"] == st["t"]
             m = np.isfinite(ref_avg)
             np.testing.assert_array_equal(avgs[i][m], ref_avg[m])
+            if i < 3:  # and the oracle's run of the same request (cell averages of the final state)
+                prob = pkg.problems.make(name)
+                o = ora.OracleSolver(n, n, p, p, 3, *prob.domain, prob.gamma, prob.bc_kind, prob.bc_state)
+                o.set_state(prob.initial_state(n, n, p)[:, :, :, 1:-1, 1:-1])
+                so = o.solve(t_end, prob.cfl)
+                assert so["steps"] == r["steps"]
+                inner = (slice(None), slice(1, -1), slice(1, -1))
+                assert rel_l1(avgs[i][inner], o.u_avg[inner]).max() <= 1e-12
+                o.close()
         st = srv.stats()
         assert st["admitted"] == st["retired"] == len(REQS) and st["rounds"] >= 1
         assert min(st[k] for k in ("admit_s", "launch_s", "wait_s", "retire_s", "idle_s")) >= 0.0
