@@ -1,14 +1,24 @@
-"""Per-degree tuning of the residual kernel on the GPU at hand.
+"""Per-degree tuning of the stage kernels on the GPU at hand.
 
-    python pp-es-dg-mhd_b200/autotune.py [--out PATH] [--jobs J]
+    python pp-es-dg-mhd_b200/autotune.py [--what residual|post|all] [--jobs J]
 
-Builds the library once per candidate set (every set gives each degree p = 1, 2, 3 one tile
-configuration TX, TY, threads, CTAs per SM -- the MHD_RES2_CFG<p> macros of csrc/residual.cuh; a
-tile holds at most (threads / 32) * (32 / (p+1)^2) elements, one lane per node), times the residual
-of each degree on a large mesh with CUDA events (each set in its own process), and writes the
-fastest configuration per degree as a header (csrc/residual2_tuned.h by default), which the next
-build picks up.  Candidates whose tile does not
-fit one CTA's shared memory fail to compile and are skipped.  Needs a GPU for the timing.
+Two groups of build-time knobs, each a macro per degree p = 1, 2, 3:
+
+  residual  MHD_RES2_CFG<p> = TX, TY, threads, CTAs per SM of the residual tile (csrc/residual.cuh;
+            a tile holds at most (threads / 32) * (32 / (p+1)^2) elements, one lane per node).
+            Timed: the residual alone, CUDA events over 20 launches.  Written to
+            csrc/residual2_tuned.h.
+  post      MHD_PP_CFG<p> = threads, CTAs per SM of the loop-1 and loop-3 kernels, and
+            MHD_SIG_CFG<p> = TX, TY, CTAs per SM of the OEDG indicator kernel (csrc/post.cuh).
+            Timed: whole device-resident SSP-RK3 steps (OEDG + LDF + PP), CUDA events over 10
+            steps, since those kernels share the step with the residual.  Written to
+            csrc/post_tuned.h.
+
+The library is built once per candidate set (set i takes candidate i of every degree), in parallel;
+each set is timed in its own process on a vortex mesh of about 33 M DOFs per degree, and the
+fastest candidate per degree is written to the group's header, which the next build picks up
+(build.py rebuilds when it changes).  A set that does not build (a tile that does not fit one CTA's
+shared memory, for instance) is skipped.  Needs a GPU for the timing.
 """
 import argparse
 import json
@@ -22,29 +32,54 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import build as B  # noqa: E402
 
-# (TX, TY, NT, MINB) per degree; set i takes candidate i of every degree
-CANDIDATES = {
-    1: [(8, 8, 256, 2), (8, 4, 128, 4), (8, 6, 192, 3), (16, 4, 256, 2)],
-    2: [(6, 4, 256, 2), (4, 3, 128, 4), (6, 3, 192, 3), (8, 3, 256, 2)],
-    3: [(4, 4, 256, 2), (4, 2, 128, 4), (4, 3, 192, 3), (8, 2, 256, 2)],
+# group -> macro(s) -> per degree the candidates; set i takes candidate i of every degree
+GROUPS = {
+    "residual": {
+        "MHD_RES2_CFG": {
+            1: [(8, 8, 256, 2), (8, 4, 128, 4), (8, 6, 192, 3), (16, 4, 256, 2)],
+            2: [(6, 4, 256, 2), (4, 3, 128, 4), (6, 3, 192, 3), (8, 3, 256, 2)],
+            3: [(4, 4, 256, 2), (4, 2, 128, 4), (4, 3, 192, 3), (8, 2, 256, 2)],
+        },
+    },
+    "post": {
+        "MHD_PP_CFG": {
+            1: [(256, 4), (128, 8), (256, 3), (192, 5)],
+            2: [(256, 4), (128, 8), (256, 3), (512, 2)],
+            3: [(256, 4), (128, 8), (256, 3), (192, 5)],
+        },
+        "MHD_SIG_CFG": {
+            1: [(8, 8, 3), (8, 4, 4), (16, 4, 3), (4, 8, 4)],
+            2: [(8, 4, 3), (4, 4, 4), (8, 2, 3), (4, 8, 3)],
+            3: [(4, 4, 2), (4, 2, 3), (4, 3, 2), (2, 4, 3)],
+        },
+    },
 }
+HEADERS = {"residual": "residual2_tuned.h", "post": "post_tuned.h"}
+CANDIDATES = GROUPS["residual"]["MHD_RES2_CFG"]  # the residual tiles (checked by the CPU tests)
 MESHES = {1: 724, 2: 512, 3: 512}  # vortex, about 33 M DOFs each
 
 
-def build_set(i, tmp):
-    hdr = os.path.join(tmp, f"cfg{i}.h")
+def nsets(group):
+    counts = {len(c) for m in GROUPS[group].values() for c in m.values()}
+    assert len(counts) == 1, "every macro of a group needs the same number of candidates"
+    return counts.pop()
+
+
+def build_set(group, i, tmp):
+    hdr = os.path.join(tmp, f"{group}{i}.h")
     with open(hdr, "w") as f:
-        for p, cands in CANDIDATES.items():
-            f.write(f"#define MHD_RES2_CFG{p} {', '.join(map(str, cands[i]))}\n")
+        for macro, per_p in GROUPS[group].items():
+            for p, cands in per_p.items():
+                f.write(f"#define {macro}{p} {', '.join(map(str, cands[i]))}\n")
     objs = []
     try:
         for src in B.SOURCES:
-            obj = os.path.join(tmp, f"set{i}_{os.path.splitext(src)[0]}.o")
+            obj = os.path.join(tmp, f"{group}{i}_{os.path.splitext(src)[0]}.o")
             cmd = [B.nvcc(), *B.NVCC_FLAGS, "-include", hdr, "-I", os.path.join(B.ROOT, "include"),
                    "-x", "cu" if src.endswith(".cu") else "c++", "-c", os.path.join(B.CSRC, src), "-o", obj]
             subprocess.run(cmd, check=True, capture_output=True)
             objs.append(obj)
-        lib = os.path.join(tmp, f"set{i}.so")
+        lib = os.path.join(tmp, f"{group}{i}.so")
         subprocess.run([B.nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib, *objs,
                         "-lcudart"], check=True, capture_output=True)
         return lib
@@ -59,6 +94,7 @@ import torch
 import __graft_entry__ as ge
 pkg = ge.load_package()
 pkg.capi.load(sys.argv[1])
+what = sys.argv[4]
 out = {}
 for p, n in json.loads(sys.argv[3]).items():
     prob = pkg.problems.make("vortex")
@@ -66,58 +102,79 @@ for p, n in json.loads(sys.argv[3]).items():
     st = torch.cuda.Stream()
     s.set_stream(st.cuda_stream)
     s.init_problem(prob)
-    s.apply_bc(0)
-    for _ in range(3):
-        s.lib.mhd_gpu_semidiscretize(s.h, 1, 0, None)
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(st):
-        e0.record(st)
-    for _ in range(20):
-        s.lib.mhd_gpu_semidiscretize(s.h, 1, 0, None)
-    with torch.cuda.stream(st):
-        e1.record(st)
-    torch.cuda.synchronize()
-    out[p] = e0.elapsed_time(e1) / 20
+    if what == "residual":
+        s.apply_bc(0)
+        for _ in range(3):
+            s.lib.mhd_gpu_semidiscretize(s.h, 1, 0, None)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(st):
+            e0.record(st)
+        for _ in range(20):
+            s.lib.mhd_gpu_semidiscretize(s.h, 1, 0, None)
+        with torch.cuda.stream(st):
+            e1.record(st)
+        torch.cuda.synchronize()
+        out[p] = e0.elapsed_time(e1) / 20
+    else:
+        s.solve_begin(prob.final_T, prob.cfl, True, True, False)
+        s.advance(3)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(st):
+            e0.record(st)
+        r = s.advance(10, check_every=10)
+        with torch.cuda.stream(st):
+            e1.record(st)
+        torch.cuda.synchronize()
+        out[p] = e0.elapsed_time(e1) / 10
     s.close()
 print(json.dumps(out))
 """
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(B.CSRC, "residual2_tuned.h"))
-    ap.add_argument("--jobs", type=int, default=4)
-    args = ap.parse_args()
-    nsets = len(CANDIDATES[1])
+def tune(group, jobs):
+    n = nsets(group)
     with tempfile.TemporaryDirectory() as tmp:
-        with ThreadPoolExecutor(args.jobs) as ex:
-            libs = list(ex.map(lambda i: build_set(i, tmp), range(nsets)))
+        with ThreadPoolExecutor(jobs) as ex:
+            libs = list(ex.map(lambda i: build_set(group, i, tmp), range(n)))
         times = {}
         for i, lib in enumerate(libs):
             if lib is None:
-                print(f"set {i}: does not build, skipped", flush=True)
+                print(f"{group} set {i}: does not build, skipped", flush=True)
                 continue
-            r = subprocess.run([sys.executable, "-c", TIMER, lib, B.ROOT, json.dumps(MESHES)],
+            r = subprocess.run([sys.executable, "-c", TIMER, lib, B.ROOT, json.dumps(MESHES), group],
                                capture_output=True, text=True)
             if r.returncode:
-                print(f"set {i}: timing failed, skipped\n{r.stderr[-400:]}", flush=True)
+                print(f"{group} set {i}: timing failed, skipped\n{r.stderr[-400:]}", flush=True)
                 continue
             times[i] = {int(p): ms for p, ms in json.loads(r.stdout.strip().splitlines()[-1]).items()}
-            print(f"set {i}: {times[i]}", flush=True)
+            print(f"{group} set {i}: {times[i]}", flush=True)
     if not times:
-        sys.exit("no candidate set could be timed")
-    lines = ["// residual2_tuned.h -- written by autotune.py: residual tile per degree, fastest of the",
-             "// candidates timed on this GPU (residual ms per launch, vortex mesh of about 33 M DOFs)."]
+        sys.exit(f"no {group} candidate set could be timed")
+    unit = "residual ms per launch" if group == "residual" else "ms per SSP-RK3 step (OEDG + LDF + PP)"
+    lines = [f"// {HEADERS[group]} -- written by autotune.py: the fastest candidate per degree on this GPU",
+             f"// ({unit}, vortex mesh of about 33 M DOFs)."]
     for p in (1, 2, 3):
         best = min(times, key=lambda i: times[i][p])
         for i in sorted(times):
-            lines.append(f"//   p={p} {CANDIDATES[p][i]}: {times[i][p]:.4f} ms{'  <- chosen' if i == best else ''}")
-        lines += [f"#ifndef MHD_RES2_CFG{p}", f"#define MHD_RES2_CFG{p} {', '.join(map(str, CANDIDATES[p][best]))}",
-                  "#endif"]
-    with open(args.out, "w") as f:
+            knobs = "; ".join(f"{m} {GROUPS[group][m][p][i]}" for m in GROUPS[group])
+            lines.append(f"//   p={p} {knobs}: {times[i][p]:.4f} ms{'  <- chosen' if i == best else ''}")
+        for macro, per_p in GROUPS[group].items():
+            lines += [f"#ifndef {macro}{p}", f"#define {macro}{p} {', '.join(map(str, per_p[p][best]))}", "#endif"]
+    path = os.path.join(B.CSRC, HEADERS[group])
+    with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
-    print(open(args.out).read())
+    print(open(path).read())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--what", default="all", choices=["residual", "post", "all"])
+    ap.add_argument("--jobs", type=int, default=4)
+    args = ap.parse_args()
+    for group in (["residual", "post"] if args.what == "all" else [args.what]):
+        tune(group, args.jobs)
+        B.build()  # the next group is timed with this group's choice built in
 
 
 if __name__ == "__main__":

@@ -304,7 +304,7 @@ void launch_diag(mhd_gpu* h, const double* u, int gate) {
   const long long E = (long long)h->nx * h->ny;
   const int nb = (int)std::min<long long>(DIAG_MAX_BLOCKS, std::max<long long>(1, E / 16));
   stage_diag_kernel<P><<<nb, 256, 0, h->stream>>>(u, h->geo, h->ctrl, gate, h->diag_part,
-                                                   reinterpret_cast<unsigned int*>(h->diag_part + 10 * DIAG_MAX_BLOCKS),
+                                                   reinterpret_cast<unsigned int*>(h->diag_part + DIAG_VALS * DIAG_MAX_BLOCKS),
                                                    h->log, h->log_cap);
 }
 
@@ -997,7 +997,7 @@ int mhd_gpu_set_log(mhd_gpu_t* h, int capacity, int diagnostics) {
   rc = device_pool(h->device, &pool);
   if (rc) return rc;
   const size_t ring = (sizeof(LogEntry) * (size_t)capacity + 255) / 256 * 256;
-  const size_t part = sizeof(double) * 10 * DIAG_MAX_BLOCKS + 256;  // partials, then the ticket
+  const size_t part = sizeof(double) * DIAG_VALS * DIAG_MAX_BLOCKS + 256;  // partials, then the ticket
   CK(cudaMallocFromPoolAsync(&h->log_block, ring + part, pool, h->stream));
   CK(cudaMemsetAsync(h->log_block, 0, ring + part, h->stream));
   rc = read_ctrl(h);  // also orders the set-up before the caller's next use

@@ -1090,13 +1090,23 @@ __global__ void __launch_bounds__(256) stage_end_bc_batched(const InstDesc* __re
 // ticket; the ticket is left at zero.
 // ---------------------------------------------------------------------------------------------
 constexpr int DIAG_MAX_BLOCKS = 592;  // 4 x 148 SMs
+constexpr int DIAG_VALS = 18;          // per block: min rho, min p, 8 sums and their 8 compensations
+
+// Neumaier's compensated summation (a running sum s and the sum c of its rounding errors): the
+// domain integrals are checked against conservation at the 1e-13 level, below the rounding error of
+// a plain sum of 10^5-10^7 terms.
+__device__ __forceinline__ void neu_add(double& s, double& c, double x) {
+  const double t = __dadd_rn(s, x);
+  c = __dadd_rn(c, fabs(s) >= fabs(x) ? __dadd_rn(__dadd_rn(s, -t), x) : __dadd_rn(__dadd_rn(x, -t), s));
+  s = t;
+}
 
 template <int P>
 __global__ void __launch_bounds__(256) stage_diag_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
                                                         double* __restrict__ part, unsigned int* ticket,
                                                         LogEntry* log, int log_cap) {
   constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
-  __shared__ double s[10][256];
+  __shared__ double s[DIAG_VALS][256];
   __shared__ bool s_last;
   if (!gate_open(ctrl, gate) || !log || log_cap <= 0 || ctrl->log_seq <= 0) return;
   const int tid = threadIdx.x;
@@ -1104,8 +1114,10 @@ __global__ void __launch_bounds__(256) stage_diag_kernel(const double* __restric
   const long long E = (long long)nx * ny;
   const long long e0 = E * blockIdx.x / gridDim.x, e1 = E * (blockIdx.x + 1) / gridDim.x;
   const DegConst& dc = c_deg[P];
-  const double gamma = g.gamma, q4 = 0.25 * g.hx * g.hy;
-  double rmin = 1.0e308, pmin = 1.0e308, acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const double gamma = g.gamma, q4 = __dmul_rn(__dmul_rn(0.25, g.hx), g.hy);
+  double rmin = 1.0e308, pmin = 1.0e308, sum[8], cmp[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) sum[v] = cmp[v] = 0.0;
   for (long long it = e0 * NN + tid; it < e1 * NN; it += 256) {
     const long long e = it / NN;
     const int q = (int)(it - e * NN), k = q % N, l = q / N;
@@ -1116,39 +1128,53 @@ __global__ void __launch_bounds__(256) stage_diag_kernel(const double* __restric
     for (int v = 0; v < 8; ++v) w[v] = x[v * NN];
     rmin = fmin(rmin, w[0]);
     pmin = fmin(pmin, prs_of(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], gamma));
-    const double wq = q4 * dc.qw[k] * dc.qw[l];
+    const double wq = __dmul_rn(__dmul_rn(q4, dc.qw[k]), dc.qw[l]);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] += wq * w[v];
+    for (int v = 0; v < 8; ++v) neu_add(sum[v], cmp[v], __dmul_rn(wq, w[v]));
   }
   s[0][tid] = rmin;
   s[1][tid] = pmin;
 #pragma unroll
-  for (int v = 0; v < 8; ++v) s[2 + v][tid] = acc[v];
+  for (int v = 0; v < 8; ++v) {
+    s[2 + v][tid] = sum[v];
+    s[10 + v][tid] = cmp[v];
+  }
   __syncthreads();
   for (int w = 128; w > 0; w >>= 1) {
     if (tid < w) {
       s[0][tid] = fmin(s[0][tid], s[0][tid + w]);
       s[1][tid] = fmin(s[1][tid], s[1][tid + w]);
 #pragma unroll
-      for (int v = 2; v < 10; ++v) s[v][tid] = s[v][tid] + s[v][tid + w];
+      for (int v = 0; v < 8; ++v) {  // (s, c) + (s', c'): the sums by Neumaier, the compensations plainly
+        double a = s[2 + v][tid], c = __dadd_rn(s[10 + v][tid], s[10 + v][tid + w]);
+        neu_add(a, c, s[2 + v][tid + w]);
+        s[2 + v][tid] = a;
+        s[10 + v][tid] = c;
+      }
     }
     __syncthreads();
   }
-  if (tid < 10) part[blockIdx.x * 10 + tid] = s[tid][0];
+  if (tid < DIAG_VALS) part[blockIdx.x * DIAG_VALS + tid] = s[tid][0];
   __threadfence();
   __syncthreads();
   if (tid == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (tid < 10) {
-    const volatile double* vp = part;
+  const volatile double* vp = part;
+  LogEntry* e = log + ((ctrl->log_seq - 1) % log_cap);
+  if (tid < 2) {
     double r = vp[tid];
-    for (unsigned b = 1; b < gridDim.x; ++b) r = tid < 2 ? fmin(r, vp[b * 10 + tid]) : r + vp[b * 10 + tid];
-    LogEntry* e = log + ((ctrl->log_seq - 1) % log_cap);
+    for (unsigned b = 1; b < gridDim.x; ++b) r = fmin(r, vp[b * DIAG_VALS + tid]);
     if (tid == 0) e->rho_min = r;
-    else if (tid == 1) e->p_min = r;
-    else e->total[tid - 2] = r;
+    else e->p_min = r;
+  } else if (tid < 10) {  // the blocks' (sum, compensation) pairs in block order
+    double a = vp[tid], c = vp[tid + 8];
+    for (unsigned b = 1; b < gridDim.x; ++b) {
+      c = __dadd_rn(c, vp[b * DIAG_VALS + tid + 8]);
+      neu_add(a, c, vp[b * DIAG_VALS + tid]);
+    }
+    e->total[tid - 2] = __dadd_rn(a, c);
   }
   if (tid == 0) *ticket = 0u;
 }

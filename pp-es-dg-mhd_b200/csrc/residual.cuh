@@ -569,14 +569,15 @@ struct Res2Layout {
   static_assert(NT % 32 == 0 && NT <= 1024, "whole warps");
   static_assert((ES * 8) % 16 == 0, "bulk copies land on 16-byte boundaries");
   static constexpr int O_CONS = 0;
-  static constexpr int O_HXL = O_CONS + TE * ES;
+  static constexpr int O_U0 = O_CONS + TE * ES;  // u_con's tile when the next stage is formed here
+  static constexpr int O_HXL = O_U0 + TE * ES;
   static constexpr int O_HXR = O_HXL + TY * 8 * N;
   static constexpr int O_HYB = O_HXR + TY * 8 * N;
   static constexpr int O_HYT = O_HYB + TX * 8 * N;
   static constexpr int O_FX = O_HYT + TX * 8 * N;
   static constexpr int O_FY = O_FX + NFX * FW;
   static constexpr int O_DM = O_FY + NFY * FW;  // D (N x N) and 1/w_k
-  static constexpr int O_RED = O_DM + NN + N;   // NW doubles of the block minimum
+  static constexpr int O_RED = O_DM + NN + N;   // NW doubles of the block minimum; [31] = the try's dt
   static constexpr int O_BAR = O_RED + 32;      // the tile's mbarrier (8 bytes)
   static constexpr int TOTAL = O_BAR + 2;
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
@@ -622,6 +623,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   constexpr int NT = L::NT, NW = L::NW, G = L::G;
   constexpr unsigned FULL = 0xffffffffu;
   double* s_cons = sm + L::O_CONS;
+  double* s_u0 = sm + L::O_U0;
   double* s_hxl = sm + L::O_HXL;
   double* s_hxr = sm + L::O_HXR;
   double* s_hyb = sm + L::O_HYB;
@@ -640,21 +642,28 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   const double gamma = g.gamma;
 
   // ---- phase 0: the tile's element blocks by bulk copies (warp 0), halo traces by loads ----
+  // (with a next-stage combination, u_con's blocks of the tile come the same way)
+  const int ncopy = sc.u0 ? 2 : 1;
   if (warp == 0) {
     if (lane == 0) {
       fence_proxy_async_smem();  // the previous tile's reads of s_cons come before these writes
-      mbar_arrive_expect_tx(bar, (unsigned)(H * W * EB * 8));
+      mbar_arrive_expect_tx(bar, (unsigned)(ncopy * H * W * EB * 8));
+      if (sc.u0) s_red[31] = *sc.dt;
     }
     __syncwarp();
-    if (ES == EB) {  // unpadded records: one copy per tile row
-      for (int r = lane; r < H; r += 32)
-        bulk_copy_g2s(s_cons + r * TX * ES, u + (long long)(j0 + r) * rowstride + (long long)i0 * EB,
-                      (unsigned)(W * EB * 8), bar);
-    } else {  // padded records: one copy per element block
-      for (int it = lane; it < H * W; it += 32) {
-        const int r = it / W, c = it - r * W;
-        bulk_copy_g2s(s_cons + (r * TX + c) * ES, u + (long long)(j0 + r) * rowstride + (long long)(i0 + c) * EB,
-                      (unsigned)(EB * 8), bar);
+    for (int which = 0; which < ncopy; ++which) {
+      const double* src = which ? sc.u0 : u;
+      double* dst = which ? s_u0 : s_cons;
+      if (ES == EB) {  // unpadded records: one copy per tile row
+        for (int r = lane; r < H; r += 32)
+          bulk_copy_g2s(dst + r * TX * ES, src + (long long)(j0 + r) * rowstride + (long long)i0 * EB,
+                        (unsigned)(W * EB * 8), bar);
+      } else {  // padded records: one copy per element block
+        for (int it = lane; it < H * W; it += 32) {
+          const int r = it / W, c = it - r * W;
+          bulk_copy_g2s(dst + (r * TX + c) * ES, src + (long long)(j0 + r) * rowstride + (long long)(i0 + c) * EB,
+                        (unsigned)(EB * 8), bar);
+        }
       }
     }
   }
@@ -767,11 +776,13 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   // the partner lane of node (kk, ll) of this lane's element
   auto lane_of = [&](int kk, int ll) { return gbase + kk + N * ll; };
   // local div B (DG_solver.f90:813), the sums in node order
+  // (every product-sum of the accumulation below is an explicit fused multiply-add, so that each
+  // kernel this tile is inlined into rounds it the same way: a batch member equals its solo run)
   double dbx = 0.0, dby = 0.0;
 #pragma unroll
-  for (int r = 0; r < N; ++r) dbx += Dm(k + N * r) * __shfl_sync(FULL, w[4], lane_of(r, l));
+  for (int r = 0; r < N; ++r) dbx = __fma_rn(Dm(k + N * r), __shfl_sync(FULL, w[4], lane_of(r, l)), dbx);
 #pragma unroll
-  for (int m = 0; m < N; ++m) dby += __shfl_sync(FULL, w[5], lane_of(k, m)) * Dm(l + N * m);
+  for (int m = 0; m < N; ++m) dby = __fma_rn(__shfl_sync(FULL, w[5], lane_of(k, m)), Dm(l + N * m), dby);
   // node flux F, G and Godunov-Powell coefficients (DG_solver.f90:749-799), formed again for the
   // surface terms after the barrier; the accumulation starts, as the reference's does
   // (DG_solver.f90:833), with the diagonal and Godunov-Powell terms
@@ -811,7 +822,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
     const double divB = sxh * dbx + syh * dby;
     const double ckk = 2.0 * sxh * Dm(k + N * k), cll = 2.0 * syh * Dm(l + N * l);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] = -(ckk * F[v]) - cll * Gf[v] - divB * GP[v];
+    for (int v = 0; v < 8; ++v) acc[v] = __fma_rn(-divB, GP[v], __fma_rn(-cll, Gf[v], -__dmul_rn(ckk, F[v])));
   }
   // This lane's flux with the node in lane `src` (x frame, or y through swap_xy); the result F is
   // in the global frame.  Every lane of the warp calls it (the shuffles need the full warp).
@@ -843,9 +854,8 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
       const double fr = __shfl_sync(FULL, F[v], src2);
-      const double t1 = own_first ? c1 * F[v] : c2 * fr, t2 = own_first ? c2 * fr : c1 * F[v];
-      acc[v] -= t1;
-      acc[v] -= t2;
+      acc[v] = __fma_rn(-(own_first ? c1 : c2), own_first ? F[v] : fr, acc[v]);
+      acc[v] = __fma_rn(-(own_first ? c2 : c1), own_first ? fr : F[v], acc[v]);
     }
   } else {
     // rings along x and y: compute with the next node, receive from the previous one
@@ -863,9 +873,8 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
       for (int v = 0; v < 8; ++v) {
         if (v == (dir == 0 ? 4 : 5)) continue;  // that component of the flux is identically zero
         const double fr = __shfl_sync(FULL, F[v], src2);
-        const double t1 = next_first ? c1 * F[v] : c2 * fr, t2 = next_first ? c2 * fr : c1 * F[v];
-        acc[v] -= t1;
-        acc[v] -= t2;
+        acc[v] = __fma_rn(-(next_first ? c1 : c2), next_first ? F[v] : fr, acc[v]);
+        acc[v] = __fma_rn(-(next_first ? c2 : c1), next_first ? fr : F[v], acc[v]);
       }
     }
     if constexpr (P == 3) {  // the pairs (k, k^2) along x and (l, l^2) along y
@@ -881,9 +890,8 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
 #pragma unroll
       for (int v = 0; v < 8; ++v) {
         const double fr = __shfl_sync(FULL, F[v], src2);
-        const double t1 = own_first ? c1 * F[v] : c2 * fr, t2 = own_first ? c2 * fr : c1 * F[v];
-        acc[v] -= t1;
-        acc[v] -= t2;
+        acc[v] = __fma_rn(-(own_first ? c1 : c2), own_first ? F[v] : fr, acc[v]);
+        acc[v] = __fma_rn(-(own_first ? c2 : c1), own_first ? fr : F[v], acc[v]);
       }
     }
   }
@@ -900,15 +908,17 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
       const bool right = (k == N - 1);
       const double* fr = s_fx + (((ec + (right ? 1 : 0)) * TY + er) * N + l);
       const double c = (right ? sxh : -sxh) * s_dm[NN + k];
+      const double jb = __dadd_rn(bx, -fr[8 * L::NFX]);
 #pragma unroll
-      for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
+      for (int v = 0; v < 8; ++v) acc[v] = __fma_rn(c, __fma_rn(GP[v], jb, __dadd_rn(F[v], -fr[v * L::NFX])), acc[v]);
     }
     if (l == 0 || l == N - 1) {
       const bool top = (l == N - 1);
       const double* fr = s_fy + (((er + (top ? 1 : 0)) * TX + ec) * N + k);
       const double c = (top ? syh : -syh) * s_dm[NN + l];
+      const double jb = __dadd_rn(by, -fr[8 * L::NFY]);
 #pragma unroll
-      for (int v = 0; v < 8; ++v) acc[v] += c * (Gf[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
+      for (int v = 0; v < 8; ++v) acc[v] = __fma_rn(c, __fma_rn(GP[v], jb, __dadd_rn(Gf[v], -fr[v * L::NFY])), acc[v]);
     }
   }
   // dt_lim of the element: the largest node speed and interface speed per direction
@@ -928,10 +938,11 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   if (act) {
     if (sc.u0) {  // the next stage's state instead of L(u)
       const long long e = ((long long)(j0 + er) * (nx + 2) + (i0 + ec)) * EB + node;
-      const double dt = *sc.dt;
+      const double dt = s_red[31];
+      const double* u0n = s_u0 + el * ES + node;
 #pragma unroll
       for (int v = 0; v < 8; ++v)
-        sc.out[e + v * NN] = __dadd_rn(__dmul_rn(sc.ca, sc.u0[e + v * NN]),
+        sc.out[e + v * NN] = __dadd_rn(__dmul_rn(sc.ca, u0n[v * NN]),
                                        __dmul_rn(sc.cb, __dadd_rn(w[v], __dmul_rn(dt, acc[v]))));
     } else {
       double* o = ut + ((long long)(j0 + er - 1) * nx + (i0 + ec - 1)) * EB + node;
@@ -942,6 +953,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   // block minimum of dt_lim -> one atomicMin
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) my_dt = fmin(my_dt, __shfl_xor_sync(FULL, my_dt, o));
+  static_assert(L::NW <= 31, "s_red[31] holds dt");
   if (lane == 0) s_red[warp] = my_dt;
   __syncthreads();
   if (tid == 0) {

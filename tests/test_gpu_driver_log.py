@@ -8,8 +8,13 @@ stage, the minimum nodal density and pressure and the domain integrals of the co
 These tests check the log against the oracle and use it to assert:
 
   * density and pressure positive after every stage;
-  * conservation of the domain integrals of rho, m, B, E to 1e-13 relative (of the integral of
-    |u|) on periodic domains, and on the outflow blast while its boundary state is still uniform;
+  * conservation of mass to 1e-13 relative (of the integral of |rho|) on periodic domains, and on
+    the outflow blast while its boundary state is still the uniform initial state.  Momentum, field
+    and energy are not conserved by the reference's method: its Godunov-Powell source
+    -divB (0, B, v, B.v) (DG_solver.f90:813,833) is non-conservative, and the oracle's integrals
+    drift (energy by 2.6e-9 relative in 26 steps of Orszag-Tang 32^2; momentum, field and energy
+    by 1e-7 to 1e-4 in 11 steps of the vortex 24^2).  Their device integrals are compared with the
+    oracle's after every step instead, at 1e-12 of the integral of |u|;
   * the total entropy non-increasing per step where the method guarantees it.  The LDF projection
     of the reference is not entropy stable: on the low-beta blast with LDF on, the oracle's
     total entropy rises in some steps (by up to 1e-3 relative on 40x40), and with LDF off it
@@ -51,6 +56,16 @@ def _l1_scale(u, p, hx, hy, w):
     return np.einsum("sklij,kl->s", np.abs(u[:, :, :, 1:-1, 1:-1]), W)
 
 
+def _integrals(u, hx, hy, w):
+    """exactly rounded domain integrals of the eight conserved variables (math.fsum of the
+    quadrature terms (hx hy / 4) w_k w_l u, formed in the device's order)"""
+    import math
+    q4 = 0.25 * hx * hy
+    W = (q4 * w[:, None]) * w[None, :]
+    x = u[:, :, :, 1:-1, 1:-1]
+    return np.array([math.fsum((x[v] * W[:, :, None, None]).ravel()) for v in range(8)])
+
+
 def test_log_has_every_stage_and_step_and_matches_the_oracle(pkg, ora):
     name, n, p, steps = "blast", 24, 2, 12
     prob, u0, g, st, recs, dropped = _run_logged(pkg, name, n, p, steps, check_every=5)
@@ -67,11 +82,11 @@ def test_log_has_every_stage_and_step_and_matches_the_oracle(pkg, ora):
         assert abs(r["t"] - ro["t"]) <= 1e-14 * ro["t"], (k, r["t"], ro["t"])
         assert abs(r["tot_ent"] - ro["tot_ent"]) <= 1e-12 * abs(ro["tot_ent"]), (k, r["tot_ent"], ro["tot_ent"])
         assert abs(r["dt_lim"] - ro["dt_lim"]) <= 1e-13 * ro["dt_lim"]
-        # PP-limited cells of the step's stages against the oracle's running total
+        # PP-limited cells of the step's stages against the oracle's count for that step (each oracle
+        # call here advances one step and counts its own stages)
         cells = sum(x["num_negcell"] for x in recs if x["kind"] == pkg.capi.LOG_STAGE and x["step"] == k + 1
                     and not x["neg_avg"])
-        prev = ref[k - 1]["num_negcell_total"] if k else 0
-        assert cells == ro["num_negcell_total"] - prev, (k, cells)
+        assert cells == ro["num_negcell_total"], (k, cells, ro["num_negcell_total"])
     assert sum(x["num_negcell"] for x in recs if x["kind"] == pkg.capi.LOG_STAGE) > 0, "limiter must act here"
     # a second read returns nothing new
     again, _ = g.read_log()
@@ -95,10 +110,10 @@ def test_log_diagnostics_match_a_host_integral(pkg):
     hx = (prob.domain[1] - prob.domain[0]) / n
     hy = (prob.domain[3] - prob.domain[2]) / n
     W = 0.25 * hx * hy * np.outer(w, w)
-    tot = np.einsum("sklij,kl->s", u0[:, :, :, 1:-1, 1:-1], W)
+    tot = _integrals(u0, hx, hy, w)
     scale = _l1_scale(u0, p, hx, hy, w)
     dev = np.array(recs[0]["total"])
-    assert np.all(np.abs(dev - tot) <= 1e-14 * scale), (dev, tot)
+    assert np.all(np.abs(dev - tot) <= 1e-15 * scale), (dev, tot)
     x = u0[:, :, :, 1:-1, 1:-1]
     prs = (prob.gamma - 1) * (x[7] - 0.5 * ((x[1] ** 2 + x[2] ** 2 + x[3] ** 2) / x[0] + (x[4] ** 2 + x[5] ** 2 + x[6] ** 2)))
     assert recs[0]["rho_min"] == x[0].min()
@@ -107,7 +122,7 @@ def test_log_diagnostics_match_a_host_integral(pkg):
 
 
 @pytest.mark.parametrize("name,n,p,steps", [("ot2pi", 128, 2, 60), ("vortex", 64, 3, 40)])
-def test_invariants_every_stage_periodic(pkg, name, n, p, steps):
+def test_invariants_every_stage_periodic(pkg, ora, name, n, p, steps):
     prob, u0, g, st, recs, dropped = _run_logged(pkg, name, n, p, steps)
     assert dropped == 0 and st["steps"] == steps and st["flags"] == 0
     w = pkg.problems.gll_nodes(p)[1]
@@ -119,13 +134,21 @@ def test_invariants_every_stage_periodic(pkg, name, n, p, steps):
     assert len(stages) == 3 * steps
     for r in stages:
         assert r["rho_min"] > 0 and r["p_min"] > 0, r
-        # every SSP stage is a convex combination of conservative updates: all eight integrals
-        # (rho, m, B, E) are conserved on a periodic domain
-        dev = np.abs(np.array(r["total"]) - t0)
-        assert np.all(dev <= 1e-13 * scale), (r["step"], r["stage"], dev / scale)
+        # every SSP stage is a convex combination of conservative updates of the density
+        assert abs(r["total"][0] - t0[0]) <= 1e-13 * scale[0], (r["step"], r["stage"], r["total"][0] - t0[0])
     ents = [r["tot_ent"] for r in recs if r["kind"] == pkg.capi.LOG_STEP]
     assert len(ents) == steps + 1
     assert all(b <= a for a, b in zip(ents, ents[1:])), np.diff(ents)
+    # the non-conserved integrals follow the oracle's step by step (the first 10 steps)
+    step_recs = [r for r in recs if r["kind"] == pkg.capi.LOG_STEP][1:]
+    o, ref = _oracle_steps(pkg, ora, prob, u0, n, p, 1)
+    for k in range(10):
+        if k:
+            o.solve(prob.final_T, prob.cfl, True, True, max_steps=1, resume=True)
+        tot = _integrals(o.u_con, hx, hy, w)
+        dev = np.array(step_recs[k]["total"])
+        assert np.all(np.abs(dev - tot) <= 1e-12 * np.maximum(scale, 1e-300) + 1e-300), (k, dev - tot)
+    o.close()
     g.close()
 
 
@@ -160,7 +183,7 @@ def test_blast400_to_final_time(pkg, ora):
     r, dropped = g.read_log()
     recs += r
     assert dropped == 0 and st["flags"] == 0 and st["done"] == 1
-    assert st["t"] == prob.final_T
+    assert abs(st["t"] - prob.final_T) <= 1e-15 * prob.final_T
     stages = [x for x in recs if x["kind"] == pkg.capi.LOG_STAGE]
     steps = [x for x in recs if x["kind"] == pkg.capi.LOG_STEP]
     assert len(steps) == st["steps"] + 1
@@ -177,11 +200,10 @@ def test_blast400_to_final_time(pkg, ora):
     h = 1.0 / n
     scale = _l1_scale(u0, p, h, h, w)
     t0 = np.array(steps[0]["total"])
-    for x in stages:
+    for x in stages:  # mass, while the boundary state is still the uniform initial state
         if x["step"] > 40 or x["neg_avg"]:
             break
-        dev = np.abs(np.array(x["total"]) - t0)
-        assert np.all(dev <= 1e-13 * scale), (x["step"], x["stage"], dev / scale)
+        assert abs(x["total"][0] - t0[0]) <= 1e-13 * scale[0], (x["step"], x["stage"], x["total"][0] - t0[0])
     g.close()
 
 

@@ -238,7 +238,7 @@ def test_ot_full_run_small(pkg, ora):
     o.set_state(u0[:, :, :, 1:-1, 1:-1])
     so = o.solve(prob.final_T, prob.cfl)
     assert sg["done"] == 1 and sg["steps"] == so["steps"]
-    assert sg["t"] == so["t"]
+    assert abs(sg["t"] - so["t"]) <= 1e-15 * so["t"]  # the clipped final step: t within an ulp or two
     err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
     assert err.max() <= 1e-10, err
     assert abs(sg["tot_ent"] - so["tot_ent"]) <= 1e-12 * abs(so["tot_ent"])
@@ -255,7 +255,7 @@ def test_ot_config_full_run(pkg, ora):
     so = o.solve(prob.final_T, prob.cfl)
     assert so["status"] == 0 and sg["flags"] == 0 and sg["done"] == 1
     assert sg["steps"] == so["steps"] and sg["retries"] == so["retries"]
-    assert sg["t"] == so["t"]
+    assert abs(sg["t"] - so["t"]) <= 1e-15 * so["t"]  # the clipped final step: t within an ulp or two
     err = rel_l1(g.download_state(0)[:, :, :, 1:-1, 1:-1], o.u_con[:, :, :, 1:-1, 1:-1])
     assert err.max() <= TOL, err
     assert abs(sg["tot_ent"] - so["tot_ent"]) <= 1e-13 * abs(so["tot_ent"])
