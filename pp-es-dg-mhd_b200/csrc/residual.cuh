@@ -614,8 +614,11 @@ __device__ __forceinline__ double group_max(double v, int gbase) {
 // One tile (elements tile_x*TX + 1 .., tile_y*TY + 1 ..).  `phase` = the parity of the tile
 // barrier's next phase (flipped here).  Returns false if the wait for the tile's copies ran out
 // (FLAG_DEVICE_WAIT is then set): the caller must stop.
+// Not inlined: every kernel (single instance, persistent, batched, allocation-free) calls this one
+// compiled copy, so the compiler's choices of fused multiply-adds are the same in all of them and a
+// batch member is bitwise equal to its solo run.  The call costs nothing measurable (once a tile).
 template <int P>
-__device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, double* __restrict__ ut,
+__device__ __noinline__ bool residual_tile2(const double* __restrict__ u, double* __restrict__ ut,
                                                const Geo& g, Ctrl* ctrl, int tile_x, int tile_y, double* sm,
                                                unsigned& phase, const StageCombine& sc = StageCombine{}) {
   using L = Res2Layout<P>;

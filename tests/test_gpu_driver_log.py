@@ -72,6 +72,8 @@ def test_log_has_every_stage_and_step_and_matches_the_oracle(pkg, ora):
     assert dropped == 0 and st["steps"] == steps and st["flags"] == 0
     o, ref = _oracle_steps(pkg, ora, prob, u0, n, p, steps)
     assert st["retries"] == ref[-1]["retries"] == 0
+    from test_gpu_parity import _ent_tol
+    ent_tol = _ent_tol(o.u_con, prob.gamma)
     # the initial record, then per try R stage records, per accepted step one step record
     assert recs[0]["kind"] == pkg.capi.LOG_STEP and recs[0]["step"] == 0 and recs[0]["t"] == 0.0
     assert [r["seq"] for r in recs] == list(range(len(recs)))
@@ -80,7 +82,9 @@ def test_log_has_every_stage_and_step_and_matches_the_oracle(pkg, ora):
     assert len(recs) == 1 + steps * (3 + 1)
     for k, (r, ro) in enumerate(zip(step_recs, ref)):
         assert abs(r["t"] - ro["t"]) <= 1e-14 * ro["t"], (k, r["t"], ro["t"])
-        assert abs(r["tot_ent"] - ro["tot_ent"]) <= 1e-12 * abs(ro["tot_ent"]), (k, r["tot_ent"], ro["tot_ent"])
+        # the total entropy's tolerance carries the conditioning of the pressure, max(E/p), as in
+        # the parity tests (about 4000 on the low-beta blast)
+        assert abs(r["tot_ent"] - ro["tot_ent"]) <= ent_tol * abs(ro["tot_ent"]), (k, r["tot_ent"], ro["tot_ent"])
         assert abs(r["dt_lim"] - ro["dt_lim"]) <= 1e-13 * ro["dt_lim"]
         # PP-limited cells of the step's stages against the oracle's count for that step (each oracle
         # call here advances one step and counts its own stages)
