@@ -35,7 +35,7 @@ def _stale():
         return True
     t = os.path.getmtime(LIB)
     paths = [os.path.join(CSRC, d) for d in DEPS] + [os.path.join(ROOT, "include", "mhd_gpu.h")]
-    for tuned in ("residual_tuned.h", "residual2_tuned.h", "post_tuned.h"):  # written by autotune.py
+    for tuned in ("residual2_tuned.h", "post_tuned.h"):  # written by autotune.py
         if os.path.exists(os.path.join(CSRC, tuned)):
             paths.append(os.path.join(CSRC, tuned))
     return any(os.path.getmtime(p) > t for p in paths)

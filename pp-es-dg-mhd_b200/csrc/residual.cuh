@@ -1,107 +1,13 @@
 // residual.cuh -- DG_semidiscretize (DG_solver.f90:663-892) as one sm_100a kernel.
 //
-// One CTA owns a TX x TY tile of interior elements.  Phases (separated by __syncthreads):
-//   0  load: tile rows are contiguous runs of element blocks -> 128-bit loads into shared
-//      memory; the four halo traces (the neighbour nodes on the tile boundary) come from the
-//      neighbouring elements (ghost ring or the next tile).
-//   1  per node: primitives (rho, v, B, beta) and the fast wave speeds.
-//   2  fluxes: every interface node of the tile gets ESPP_HLL_flux_x once (the y faces through
-//      swap_xy), and every element node pair along x and y gets its entropy-conservative flux
-//      once (the reference's symmetric r<k / s<l scatter, DG_solver.f90:833-848).
-//   3  per node: diagonal volume term, Godunov-Powell source with the local div B, the pair
-//      contributions in a fixed order, and the surface terms; per element: dt_lim.
-//   4  store: ut tile rows back with 128-bit stores; block min of dt_lim -> one atomicMin.
-// Work items of a phase are spread over the CTA's threads round-robin.  Sums are formed in a
-// fixed order, so the kernel is deterministic.
+// ut = L(u): the entropy-conservative two-point flux differencing over the GLL nodes of each
+// element, the ESPP-HLL interface flux, the Godunov-Powell source and the surface terms, and
+// dt_lim.  One CTA owns a tile of elements; one lane owns one node (see residual_tile2 below).
+// Sums are formed in a fixed order, so the kernel is deterministic.
 #pragma once
 #include "common.cuh"
 
 namespace mhd {
-
-// Tile (TX x TY elements), threads per CTA and the CTAs per SM the register budget is cut for.
-template <int P>
-struct ResCfg;
-// MHD_RES_CFG<p> = TX, TY, NT, MINB, HW, where HW = warps that start phase 2 on the interface
-// fluxes (all warps then share the node pairs through a shared-memory work counter).  The values
-// below were chosen by timing on B200.  autotune.py (next to build.py) times candidate sets on the
-// GPU at hand and writes residual_tuned.h, which takes precedence when present.
-#if __has_include("residual_tuned.h")
-#include "residual_tuned.h"
-#endif
-#ifndef MHD_RES_CFG1
-#define MHD_RES_CFG1 8, 4, 128, 4, 3
-#endif
-#ifndef MHD_RES_CFG2
-#define MHD_RES_CFG2 4, 4, 128, 4, 2
-#endif
-#ifndef MHD_RES_CFG3
-#define MHD_RES_CFG3 4, 2, 128, 4, 3
-#endif
-struct ResParams {
-  int TX, TY, NT, MINB, HW;
-};
-template <>
-struct ResCfg<1> {
-  static constexpr ResParams c{MHD_RES_CFG1};
-  static constexpr int TX = c.TX, TY = c.TY, NT = c.NT, MINB = c.MINB, HW = c.HW;
-};
-template <>
-struct ResCfg<2> {
-  static constexpr ResParams c{MHD_RES_CFG2};
-  static constexpr int TX = c.TX, TY = c.TY, NT = c.NT, MINB = c.MINB, HW = c.HW;
-};
-template <>
-struct ResCfg<3> {
-  static constexpr ResParams c{MHD_RES_CFG3};
-  static constexpr int TX = c.TX, TY = c.TY, NT = c.NT, MINB = c.MINB, HW = c.HW;
-};
-
-template <int P>
-struct ResLayout {
-  static constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
-  // shared element records padded by 16 bytes for p = 1 and 3, so that the same node of
-  // neighbouring elements falls in different banks (face traces are read across elements); at
-  // p = 2 the unpadded 576-byte record measured faster
-  static constexpr int ES = EB + (P == 2 ? 0 : 2);
-  static constexpr int TX = ResCfg<P>::TX, TY = ResCfg<P>::TY, TE = TX * TY;
-  static constexpr int NPR = N * (N - 1) / 2;  // pairs per line
-  static constexpr int NPX = N * NPR;          // x pairs per element
-  static constexpr int NPAIR = 2 * NPX;
-  static constexpr int NFX = (TX + 1) * TY * N;
-  static constexpr int NFY = TX * (TY + 1) * N;
-  static constexpr int FW = 11;  // face record: flux[8], nB, sl, sr (stored component-major)
-  static constexpr int THL = 32 * ResCfg<P>::HW;  // threads that start phase 2 on the face nodes
-  static_assert(ResCfg<P>::HW >= 1 && THL <= ResCfg<P>::NT, "face warps must fit the CTA");
-  // offsets in doubles
-  static constexpr int O_CONS = 0;
-  static constexpr int O_PRIM = O_CONS + TE * ES;
-  static constexpr int O_HXL = O_PRIM + TE * ES;
-  static constexpr int O_HXR = O_HXL + TY * 8 * N;
-  static constexpr int O_HYB = O_HXR + TY * 8 * N;
-  static constexpr int O_HYT = O_HYB + TX * 8 * N;
-  static constexpr int O_FX = O_HYT + TX * 8 * N;
-  static constexpr int O_FY = O_FX + NFX * FW;
-  static constexpr int O_PAIR = O_FY + NFY * FW;
-  static constexpr int O_SIG = O_PAIR + TE * NPAIR * 8;
-  static constexpr int O_PT = O_SIG + TE * 2 * NN;  // total pressure p + |B|^2/2 per node
-  static constexpr int O_RED = O_PT + TE * NN;
-  static constexpr int O_DM = O_RED + 32;  // O_RED + 16 doubles also hold the pair work counter
-  static constexpr int TOTAL = O_DM + NN + N;  // D (N x N) and 1/w_k of this degree
-  static constexpr size_t BYTES = sizeof(double) * TOTAL;
-  static_assert(BYTES <= 227 * 1024, "residual tile does not fit the shared memory of one CTA");
-  static_assert(ResCfg<P>::NT % 32 == 0 && ResCfg<P>::NT <= 512, "whole warps, at most 16");
-};
-
-// pair index within a line -> (a, b), b < a, enumerated a = 1..N-1, b = 0..a-1
-__device__ __forceinline__ void pair_ab(int idx, int& a, int& b) {
-  a = 1;
-  while (idx >= a) {
-    idx -= a;
-    ++a;
-  }
-  b = idx;
-}
-__device__ __forceinline__ int pair_index(int a, int b) { return a * (a - 1) / 2 + b; }
 
 // swap_xy (DG_solver.f90:1556-1568) as a variable permutation: 1 <-> 2, 4 <-> 5
 __host__ __device__ constexpr int swap_xy_var(int v) { return v == 1 ? 2 : v == 2 ? 1 : v == 4 ? 5 : v == 5 ? 4 : v; }
@@ -116,391 +22,6 @@ struct StageCombine {
   double ca, cb;
   const double* dt;     // the try's dt (device control block)
 };
-
-// One tile of the residual: elements (tile_x*TX + 1 .. , tile_y*TY + 1 .. ) of the instance
-// described by (u, ut, g, ctrl).  All threads of the CTA call it with the same arguments.
-template <int P>
-__device__ __forceinline__ void residual_tile(const double* __restrict__ u, double* __restrict__ ut,
-                                              const Geo& g, Ctrl* ctrl, int tile_x, int tile_y,
-                                              double* sm, const StageCombine& sc = StageCombine{}) {
-  using L = ResLayout<P>;
-  constexpr int N = L::N, NN = L::NN, EB = L::EB, ES = L::ES, TX = L::TX, TY = L::TY, TE = L::TE;
-  constexpr int NT = ResCfg<P>::NT;
-  double* s_cons = sm + L::O_CONS;
-  double* s_prim = sm + L::O_PRIM;
-  double* s_hxl = sm + L::O_HXL;
-  double* s_hxr = sm + L::O_HXR;
-  double* s_hyb = sm + L::O_HYB;
-  double* s_hyt = sm + L::O_HYT;
-  double* s_fx = sm + L::O_FX;
-  double* s_fy = sm + L::O_FY;
-  double* s_pair = sm + L::O_PAIR;
-  double* s_sig = sm + L::O_SIG;
-  double* s_pt = sm + L::O_PT;
-  double* s_red = sm + L::O_RED;
-  // Phase 3 indexes D and 1/w by node, so a warp reads several addresses at once: a constant-
-  // memory read is replayed per distinct address, a shared-memory read is not.  Measured on B200:
-  // faster from shared memory at p = 3 (0.8 %), slower at p = 1, equal at p = 2.
-  constexpr bool DM_SHARED = (P == 3);
-  double* s_dm = sm + L::O_DM;
-  int* s_next = reinterpret_cast<int*>(s_red + 16);  // next node-pair chunk of phase 2
-
-  const int tid = threadIdx.x;
-  const int nx = g.nx, ny = g.ny;
-  const int i0 = 1 + tile_x * TX, j0 = 1 + tile_y * TY;  // first interior element
-  const int W = min(TX, nx - i0 + 1), H = min(TY, ny - j0 + 1);
-  const long long rowstride = (long long)(nx + 2) * EB;
-  const double gamma = g.gamma;
-
-  // ---- phase 0: load the tile and its halo traces ----
-  const DegConst& dc = c_deg[P];
-  if (tid == 0) *s_next = 0;
-  if (DM_SHARED && tid < NN) s_dm[tid] = dc.D[tid];
-  if (DM_SHARED && tid < N) s_dm[NN + tid] = dc.iqw[tid];
-  auto Dm = [&](int i) { return DM_SHARED ? s_dm[i] : dc.D[i]; };
-  auto iqw = [&](int i) { return DM_SHARED ? s_dm[NN + i] : dc.iqw[i]; };
-  {
-    constexpr int V2 = TX * EB / 2;  // double2 per tile row
-    for (int it = tid; it < H * V2; it += NT) {
-      const int r = it / V2, c = it - r * V2;
-      if (c < W * EB / 2) {
-        const double2* src = reinterpret_cast<const double2*>(u + (long long)(j0 + r) * rowstride + (long long)i0 * EB);
-        const int ec = (ES == EB) ? 0 : c / (EB / 2), cw = c - ec * (EB / 2);  // unpadded: one run
-        reinterpret_cast<double2*>(s_cons + (r * TX + ec) * ES)[cw] = __ldg(src + c);
-      }
-    }
-    for (int it = tid; it < TY * 8 * N; it += NT) {  // x halos: traces k = n-1 (left) / 0 (right)
-      const int r = it / (8 * N), rem = it - r * 8 * N, v = rem / N, l = rem - v * N;
-      if (r < H) {
-        const double* rowp = u + (long long)(j0 + r) * rowstride;
-        s_hxl[it] = __ldg(rowp + (long long)(i0 - 1) * EB + v * NN + (N - 1) + N * l);
-        s_hxr[it] = __ldg(rowp + (long long)(i0 + W) * EB + v * NN + 0 + N * l);
-      }
-    }
-    for (int it = tid; it < TX * 8 * N; it += NT) {  // y halos: traces l = n-1 (bottom) / 0 (top)
-      const int c = it / (8 * N), rem = it - c * 8 * N, v = rem / N, k = rem - v * N;
-      if (c < W) {
-        s_hyb[it] = __ldg(u + (long long)(j0 - 1) * rowstride + (long long)(i0 + c) * EB + v * NN + k + N * (N - 1));
-        s_hyt[it] = __ldg(u + (long long)(j0 + H) * rowstride + (long long)(i0 + c) * EB + v * NN + k);
-      }
-    }
-  }
-  __syncthreads();
-
-  // ---- phase 1: primitives and node wave speeds ----
-  for (int it = tid; it < TE * NN; it += NT) {
-    const int e = it / NN, q = it - e * NN;
-    const int er = e / TX, ec = e - er * TX;
-    if (er >= H || ec >= W) continue;
-    const double* w0 = s_cons + e * ES + q;
-    double w[8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) w[v] = w0[v * NN];
-    const double ir = 1.0 / w[0];
-    const double vx = ir * w[1], vy = ir * w[2], vz = ir * w[3];
-    const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
-    const double bsq = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
-    const double pf = fmax((gamma - 1.0) * (w[7] - (ek + 0.5 * bsq)), PP_EPS);
-    double* pr = s_prim + e * ES + q;
-    pr[0 * NN] = w[0];
-    pr[1 * NN] = vx;
-    pr[2 * NN] = vy;
-    pr[3 * NN] = vz;
-    pr[4 * NN] = w[4];
-    pr[5 * NN] = w[5];
-    pr[6 * NN] = w[6];
-    pr[7 * NN] = 0.5 * w[0] / pf;
-    const double cs = gamma * pf * ir, ss = cs + bsq * ir, coef = 4.0 * cs * ir;
-    s_pt[e * NN + q] = pf + 0.5 * bsq;
-    s_sig[e * 2 * NN + q] = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
-    s_sig[e * 2 * NN + NN + q] = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
-  }
-  __syncthreads();
-
-  // ---- phase 2: interface fluxes and element pair fluxes ----
-  // The first THL threads (whole warps) take the face nodes; all warps take the node pairs in
-  // chunks of 32 from a shared counter (the face warps once their faces are done), so the two
-  // kinds of work balance whatever their relative cost.
-  {
-    constexpr int NH = L::NFX + L::NFY, NPT = TE * L::NPAIR;
-    const double igm1 = 1.0 / (gamma - 1.0);
-    constexpr int THL = L::THL;
-    // One call site per flux: a y face or y pair is rotated into the x frame by swap_xy (the
-    // component permutation 1<->2, 4<->5, its own inverse) on the way in and out, as the
-    // reference does for faces (DG_solver.f90:1556-1568); both fluxes are exactly covariant
-    // under it, so the result equals the y-direction formula bit for bit.
-    auto face_node = [&](int it) {
-      const bool ydir = it >= L::NFX;
-      const double *pl, *pr;
-      int sl, sr;  // variable strides of the two traces
-      double* dst;
-      int ostride;
-      if (!ydir) {  // x face node: left/right traces of row r, face fi, node l
-        const int fi = it / (TY * N), rem = it - fi * TY * N, r = rem / N, l = rem - r * N;
-        if (r >= H || fi > W) return;
-        if (fi == 0) { pl = s_hxl + r * 8 * N + l; sl = N; }
-        else { pl = s_cons + (r * TX + fi - 1) * ES + (N - 1) + N * l; sl = NN; }
-        if (fi == W) { pr = s_hxr + r * 8 * N + l; sr = N; }
-        else { pr = s_cons + (r * TX + fi) * ES + N * l; sr = NN; }
-        dst = s_fx + it;
-        ostride = L::NFX;
-      } else {  // y face node: bottom/top traces of column c, face fj, node k
-        const int f = it - L::NFX;
-        const int fj = f / (TX * N), rem = f - fj * TX * N, c = rem / N, k = rem - c * N;
-        if (c >= W || fj > H) return;
-        if (fj == 0) { pl = s_hyb + c * 8 * N + k; sl = N; }
-        else { pl = s_cons + ((fj - 1) * TX + c) * ES + k + N * (N - 1); sl = NN; }
-        if (fj == H) { pr = s_hyt + c * 8 * N + k; sr = N; }
-        else { pr = s_cons + (fj * TX + c) * ES + k; sr = NN; }
-        dst = s_fy + f;
-        ostride = L::NFY;
-      }
-      double wl[8], wr[8], o[11];
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        const int sv = ydir ? swap_xy_var(v) : v;
-        wl[v] = pl[sv * sl];
-        wr[v] = pr[sv * sr];
-      }
-      espp_hll(wl, wr, gamma, igm1, o);
-#pragma unroll
-      for (int c = 0; c < L::FW; ++c) dst[(ydir && c < 8 ? swap_xy_var(c) : c) * ostride] = o[c];  // component-major
-    };
-    auto node_pair = [&](int pidx) {  // element node pair
-      const int e = pidx / L::NPAIR, pi = pidx - e * L::NPAIR;
-      const int er = e / TX, ec = e - er * TX;
-      if (er >= H || ec >= W) return;
-      const bool ydir = pi >= L::NPX;
-      const int pj = ydir ? pi - L::NPX : pi;
-      const int line = pj / L::NPR;
-      int a, b;
-      pair_ab(pj - line * L::NPR, a, b);
-      // x pair on line l: nodes (a,l) [the reference's k] and (b,l) [r];
-      // y pair on column k: nodes (k,a) [the reference's l] and (k,b) [s]
-      const double* pb = s_prim + e * ES;
-      const double* pA = pb + (ydir ? line + N * a : a + N * line);
-      const double* pB = pb + (ydir ? line + N * b : b + N * line);
-      double A[8], B[8], F[8];
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        const int sv = ydir ? swap_xy_var(v) : v;
-        A[v] = pA[sv * NN];
-        B[v] = pB[sv * NN];
-      }
-      ec_flux<0>(A, B, igm1, F);
-      double* dst = s_pair + e * L::NPAIR + pi;  // variable-major: no bank conflicts
-#pragma unroll
-      for (int v = 0; v < 8; ++v) dst[(ydir ? swap_xy_var(v) : v) * TE * L::NPAIR] = F[v];
-    };
-    if (tid < THL)
-      for (int it = tid; it < NH; it += THL) face_node(it);
-    for (;;) {
-      int base = 0;
-      if ((tid & 31) == 0) base = atomicAdd(s_next, 32);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (base >= NPT) break;
-      if (base + (tid & 31) < NPT) node_pair(base + (tid & 31));
-    }
-  }
-  __syncthreads();
-
-  // ---- phase 3: assemble ut per node; dt_lim per element ----
-  const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
-  double my_dt = 1.0e300;
-  for (int it = tid; it < TE * NN + TE; it += NT) {
-    if (it < TE * NN) {
-      const int e = it / NN, q = it - e * NN;
-      const int er = e / TX, ec = e - er * TX;
-      if (er >= H || ec >= W) continue;
-      const int k = q % N, l = q / N;
-      double* cw = s_cons + e * ES + q;
-      const double* pb = s_prim + e * ES;
-      double w[8];
-#pragma unroll
-      for (int v = 0; v < 8; ++v) w[v] = cw[v * NN];
-      // node flux F, G and Godunov-Powell coefficients (DG_solver.f90:749-799); the velocities
-      // and the total pressure are the node's phase-1 values
-      const double vx = pb[1 * NN + q], vy = pb[2 * NN + q], vz = pb[3 * NN + q];
-      const double bx = w[4], by = w[5], bz = w[6];
-      const double pt = s_pt[e * NN + q];
-      const double bu = bx * vx + by * vy + bz * vz;
-      const double ex = by * vz - bz * vy, ey = bz * vx - bx * vz, ez = bx * vy - by * vx;
-      double F[8], G[8], GP[8];
-      F[0] = w[1];
-      F[1] = vx * w[1] - bx * bx + pt;
-      F[2] = vx * w[2] - by * bx;
-      F[3] = vx * w[3] - bz * bx;
-      F[4] = 0.0;
-      F[5] = -ez;
-      F[6] = ey;
-      F[7] = vx * (w[7] + pt) - bx * bu;
-      G[0] = w[2];
-      G[1] = vy * w[1] - bx * by;
-      G[2] = vy * w[2] - by * by + pt;
-      G[3] = vy * w[3] - bz * by;
-      G[4] = ez;
-      G[5] = 0.0;
-      G[6] = -ex;
-      G[7] = vy * (w[7] + pt) - by * bu;
-      GP[0] = 0.0;
-      GP[1] = bx;
-      GP[2] = by;
-      GP[3] = bz;
-      GP[4] = vx;
-      GP[5] = vy;
-      GP[6] = vz;
-      GP[7] = bu;
-      // local div B (DG_solver.f90:813)
-      double dbx = 0.0, dby = 0.0;
-#pragma unroll
-      for (int r = 0; r < N; ++r) dbx += Dm(k + N * r) * pb[4 * NN + r + N * l];
-#pragma unroll
-      for (int m = 0; m < N; ++m) dby += pb[5 * NN + k + N * m] * Dm(l + N * m);
-      const double divB = sxh * dbx + syh * dby;
-      double acc[8];
-      const double ckk = 2.0 * sxh * Dm(k + N * k), cll = 2.0 * syh * Dm(l + N * l);
-#pragma unroll
-      for (int v = 0; v < 8; ++v) acc[v] = -(ckk * F[v]) - cll * G[v] - divB * GP[v];
-      // pair contributions along x (line l) and y (column k)
-      const double* pe = s_pair + e * L::NPAIR;
-      constexpr int PS = TE * L::NPAIR;  // stride between variables
-#pragma unroll
-      for (int r = 0; r < N; ++r) {
-        if (r == k) continue;
-        const int pi = l * L::NPR + pair_index(max(k, r), min(k, r));
-        const double c = 2.0 * sxh * Dm(k + N * r);
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
-      }
-#pragma unroll
-      for (int m = 0; m < N; ++m) {
-        if (m == l) continue;
-        const int pi = L::NPX + k * L::NPR + pair_index(max(l, m), min(l, m));
-        const double c = 2.0 * syh * Dm(l + N * m);
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] -= c * pe[v * PS + pi];
-      }
-      // surface terms (DG_solver.f90:872-882): the left face (k = 0) enters with -, the right
-      // face (k = N-1) with +; likewise bottom/top in y.  One block per direction.
-      if (k == 0 || k == N - 1) {
-        const bool right = (k == N - 1) && (N > 1);
-        const double* fr = s_fx + (((ec + (right ? 1 : 0)) * TY + er) * N + l);
-        const double c = (right ? sxh : -sxh) * iqw(k);
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] += c * (F[v] - fr[v * L::NFX] + GP[v] * (bx - fr[8 * L::NFX]));
-      }
-      if (l == 0 || l == N - 1) {
-        const bool top = (l == N - 1) && (N > 1);
-        const double* fr = s_fy + (((er + (top ? 1 : 0)) * TX + ec) * N + k);
-        const double c = (top ? syh : -syh) * iqw(l);
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[v] += c * (G[v] - fr[v * L::NFY] + GP[v] * (by - fr[8 * L::NFY]));
-      }
-      if (sc.u0) {  // the next stage's state instead of L(u)
-        const double* u0n = sc.u0 + (((long long)(j0 + er) * (nx + 2)) + (i0 + ec)) * EB + q;
-        const double dt = *sc.dt;
-#pragma unroll
-        for (int v = 0; v < 8; ++v)
-          acc[v] = __dadd_rn(__dmul_rn(sc.ca, u0n[v * NN]), __dmul_rn(sc.cb, __dadd_rn(w[v], __dmul_rn(dt, acc[v]))));
-      }
-#pragma unroll
-      for (int v = 0; v < 8; ++v) cw[v * NN] = acc[v];  // own node only: safe in place
-    } else {
-      const int e = it - TE * NN;
-      const int er = e / TX, ec = e - er * TX;
-      if (er >= H || ec >= W) continue;
-      double sx = 0.0, sy = 0.0;
-      for (int q = 0; q < NN; ++q) {
-        sx = fmax(sx, s_sig[e * 2 * NN + q]);
-        sy = fmax(sy, s_sig[e * 2 * NN + NN + q]);
-      }
-      double mxr = -1.0e300, mnl = 1.0e300, myu = -1.0e300, mnd = 1.0e300;
-      for (int l = 0; l < N; ++l) {
-        mxr = fmax(mxr, s_fx[10 * L::NFX + (ec * TY + er) * N + l]);
-        mnl = fmin(mnl, s_fx[9 * L::NFX + ((ec + 1) * TY + er) * N + l]);
-      }
-      for (int k = 0; k < N; ++k) {
-        myu = fmax(myu, s_fy[10 * L::NFY + (er * TX + ec) * N + k]);
-        mnd = fmin(mnd, s_fy[9 * L::NFY + ((er + 1) * TX + ec) * N + k]);
-      }
-      const double ax = fmax(fmax(sx, mxr), -mnl), ay = fmax(fmax(sy, myu), -mnd);
-      const double dtl = 1.0 / ((2 * P + 1) * ax / g.hx + (2 * P + 1) * ay / g.hy);
-      my_dt = fmin(my_dt, dtl);
-    }
-  }
-  // block min of dt_lim
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) my_dt = fmin(my_dt, __shfl_xor_sync(0xffffffffu, my_dt, o));
-  if ((tid & 31) == 0) s_red[tid >> 5] = my_dt;
-  __syncthreads();
-  if (tid == 0) {
-    double m = s_red[0];
-    for (int w = 1; w < NT / 32; ++w) m = fmin(m, s_red[w]);
-    atomicMin(&ctrl->dt_lim_bits, (unsigned long long)__double_as_longlong(m));
-  }
-
-  // ---- phase 4: store ut ----
-  {
-    constexpr int V2 = TX * EB / 2;
-    for (int it = tid; it < H * V2; it += NT) {
-      const int r = it / V2, c = it - r * V2;
-      if (c < W * EB / 2) {
-        double2* dst = sc.u0 ? reinterpret_cast<double2*>(sc.out + ((long long)(j0 + r) * (nx + 2) + i0) * EB)
-                             : reinterpret_cast<double2*>(ut + ((long long)(j0 + r - 1) * nx + (i0 - 1)) * EB);
-        const int ec = (ES == EB) ? 0 : c / (EB / 2), cw = c - ec * (EB / 2);
-        dst[c] = reinterpret_cast<const double2*>(s_cons + (r * TX + ec) * ES)[cw];
-      }
-    }
-  }
-}
-
-// single instance: one CTA per tile
-template <int P>
-__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
-    residual_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
-                    StageCombine sc) {
-  if (!gate_open(ctrl, gate)) return;
-  extern __shared__ __align__(16) double sm[];
-  residual_tile<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, sc);
-}
-
-// single instance, persistent: CTA b computes tiles b, b + gridDim.x, ... (row-major, ntx per row).
-// For a launch that is usually gated off (the re-try residual of every try): a grid of resident
-// CTAs that return at once costs far less than one CTA per tile.
-template <int P>
-__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
-    residual_persistent(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
-                        int ntx, int ntiles) {
-  if (!gate_open(ctrl, gate)) return;
-  extern __shared__ __align__(16) double sm[];
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    residual_tile<P>(u, ut, g, ctrl, t % ntx, t / ntx, sm, StageCombine{});
-    __syncthreads();  // the next tile reuses shared memory
-  }
-}
-
-// many instances of degree P: a persistent grid walks every member's tiles (row-major per member);
-// the state is slot `src`, the result goes to ut[dst], or (next_stage > 0) the combination of
-// stage next_stage goes to slot next_stage
-template <int P>
-__global__ void __launch_bounds__(ResCfg<P>::NT, ResCfg<P>::MINB)
-    residual_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
-                     const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate,
-                     int next_stage, double ca, double cb) {
-  extern __shared__ __align__(16) double sm[];
-  const int nw = *nwork, n = *ninst;
-  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
-    const int m = it.m, local = it.local();
-    const InstDesc& d = insts[m];
-    if (!gate_open(d.ctrl, gate)) continue;
-    const int ntx = (d.g.nx + ResCfg<P>::TX - 1) / ResCfg<P>::TX;
-    // next_stage > 0: that stage's combination is folded in (the group's rknstg is uniform)
-    const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
-    residual_tile<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, sc);
-    __syncthreads();  // the next tile reuses shared memory
-  }
-}
-
 
 // =============================================================================================
 // Node-per-lane form of the residual.
