@@ -149,6 +149,7 @@ __device__ __forceinline__ int batch_member(const int* __restrict__ pref, int n,
 // group's nw items (CTA b of G), visited in order.  The member is found by binary search once and
 // then walked forward, so consecutive items of one member reuse its descriptor (and whatever the
 // kernel staged for it), and neighbouring tiles of a member are processed close in time.
+// pref == nullptr: a single instance owns all nw items.
 struct BatchWalk {
   const int* pref;
   int w, last, m, mstart, mend;
@@ -156,8 +157,9 @@ struct BatchWalk {
     const long long b = blockIdx.x, G = gridDim.x;
     w = (int)(b * nw / G);
     last = (int)((b + 1) * nw / G);
-    m = mstart = mend = 0;
-    if (w < last) {
+    m = mstart = 0;
+    mend = nw;
+    if (pref && w < last) {
       m = batch_member(pref, n, w);
       mstart = __ldg(pref + m);
       mend = __ldg(pref + m + 1);

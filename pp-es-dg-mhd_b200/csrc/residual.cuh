@@ -135,11 +135,8 @@ __device__ __forceinline__ double group_max(double v, int gbase) {
 // One tile (elements tile_x*TX + 1 .., tile_y*TY + 1 ..).  `phase` = the parity of the tile
 // barrier's next phase (flipped here).  Returns false if the wait for the tile's copies ran out
 // (FLAG_DEVICE_WAIT is then set): the caller must stop.
-// Not inlined: every kernel (single instance, persistent, batched, allocation-free) calls this one
-// compiled copy, so the compiler's choices of fused multiply-adds are the same in all of them and a
-// batch member is bitwise equal to its solo run.  The call costs nothing measurable (once a tile).
 template <int P>
-__device__ __noinline__ bool residual_tile2(const double* __restrict__ u, double* __restrict__ ut,
+__device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, double* __restrict__ ut,
                                                const Geo& g, Ctrl* ctrl, int tile_x, int tile_y, double* sm,
                                                unsigned& phase, const StageCombine& sc = StageCombine{}) {
   using L = Res2Layout<P>;
@@ -488,50 +485,48 @@ __device__ __noinline__ bool residual_tile2(const double* __restrict__ u, double
   return true;
 }
 
-// single instance: one CTA per tile
+// The residual kernel, for every use: a single instance (insts == nullptr; its pointers, geometry
+// and next-stage combination are the one_* arguments and it has one_items tiles) or the members of a
+// batch group (the device table insts / pref / nwork / ninst; the state is slot src, the result
+// goes to ut[dst], or (next_stage > 0) the combination of stage next_stage goes to slot
+// next_stage).  The CTAs take contiguous shares of the items (tiles, row-major per member): a grid
+// of one CTA per tile for a plain launch, a persistent grid of the resident CTAs for the usually
+// gated re-try launch and for batches.  There is one call of residual_tile2 in one kernel, so every
+// use runs the same compiled arithmetic: a batch member is bitwise equal to its solo run.
 template <int P>
 __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
-    residual2_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
-                     StageCombine sc) {
-  if (!gate_open(ctrl, gate)) return;
+    residual2_kernel(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                     const int* __restrict__ nwork, const int* __restrict__ ninst, const double* one_u,
+                     double* one_ut, Geo one_g, Ctrl* one_ctrl, StageCombine one_sc, int one_items, int src,
+                     int dst, int gate, int next_stage, double ca, double cb) {
+  if (!insts && !gate_open(one_ctrl, gate)) return;
   extern __shared__ __align__(16) double sm[];
   res2_prologue<P>(sm);
   unsigned phase = 0;
-  residual_tile2<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, phase, sc);
-}
-
-// single instance, persistent (tiles b, b + gridDim.x, ..., row-major with ntx per row)
-template <int P>
-__global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
-    residual2_persistent(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
-                         int ntx, int ntiles) {
-  if (!gate_open(ctrl, gate)) return;
-  extern __shared__ __align__(16) double sm[];
-  res2_prologue<P>(sm);
-  unsigned phase = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    if (!residual_tile2<P>(u, ut, g, ctrl, t % ntx, t / ntx, sm, phase, StageCombine{})) return;
-    __syncthreads();  // the next tile reuses shared memory
-  }
-}
-
-// many instances of degree P (see residual_batched)
-template <int P>
-__global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
-    residual2_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
-                      const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate,
-                      int next_stage, double ca, double cb) {
-  extern __shared__ __align__(16) double sm[];
-  res2_prologue<P>(sm);
-  unsigned phase = 0;
-  const int nw = *nwork, n = *ninst;
-  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
-    const int m = it.m, local = it.local();
-    const InstDesc& d = insts[m];
-    if (!gate_open(d.ctrl, gate)) continue;
-    const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
-    const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
-    if (!residual_tile2<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc)) return;
+  const int nw = insts ? *nwork : one_items, n = insts ? *ninst : 1;
+  for (BatchWalk it(insts ? pref : nullptr, n, nw); it.more(); it.next()) {
+    const double* u;
+    double* ut;
+    Geo g;
+    Ctrl* ctrl;
+    StageCombine sc{};
+    if (insts) {
+      const InstDesc& d = insts[it.m];
+      u = d.u[src];
+      ut = d.ut[dst];
+      g = d.g;
+      ctrl = d.ctrl;
+      if (next_stage > 0) sc = StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt};
+    } else {
+      u = one_u;
+      ut = one_ut;
+      g = one_g;
+      ctrl = one_ctrl;
+      sc = one_sc;
+    }
+    if (!gate_open(ctrl, gate)) continue;
+    const int ntx = (g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX, local = it.local();
+    if (!residual_tile2<P>(u, ut, g, ctrl, local % ntx, local / ntx, sm, phase, sc)) return;
     __syncthreads();  // the next tile reuses shared memory
   }
 }
