@@ -198,7 +198,7 @@ template <int P>
 BatchGrids batch_grids(int nsm) {
   constexpr int EB = 8 * (P + 1) * (P + 1);
   BatchGrids gr;
-  gr.res = full_grid(residual2_kernel<P>, Res2Layout<P>::NT, Res2Layout<P>::BYTES, nsm);
+  gr.res = full_grid(residual2_batched<P>, Res2Layout<P>::NT, Res2Layout<P>::BYTES, nsm);
   gr.cmb = full_grid(combine_batched<EB>, 256, 0, nsm);
   gr.bc = full_grid(bc_batched<P>, 256, 0, nsm);
   gr.avg = full_grid(pp_avg_ldf_batched<P, false>, PPCfg<P>::NT, 0, nsm);
@@ -221,8 +221,8 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
   const int grid_res = gr.res, grid_cmb = gr.cmb, grid_bc = gr.bc, grid_avg = gr.avg, grid_sig = gr.sig,
             grid_lim = gr.lim;
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_BEGIN, R, 0);
-  residual2_kernel<P><<<grid_res, NT_RES, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, nullptr, nullptr, Geo{},
-                                                       nullptr, StageCombine{}, 0, 0, 1, ST_RECOMPUTE, 0, 0.0, 0.0);
+  residual2_batched<P><<<grid_res, NT_RES, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, 0, 1, ST_RECOMPUTE,
+                                                        0, 0.0, 0.0);
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_DT_STAGE1, R, 1);  // dt, and the pseudo-time of stage 1
   for (int s = 1; s <= R; ++s) {
     const int fin = (s == R);
@@ -249,8 +249,8 @@ void enqueue_group_try(mhd_batch* b, BatchGroup& g, const BatchGrids& gr, cudaSt
     const int nxt = (!fin && (R == 2 || R == 3)) ? s + 1 : 0;
     const double ca = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.75 : 1.0 / 3.0));
     const double cb = nxt == 0 ? 0.0 : (R == 2 ? 0.5 : (nxt == 2 ? 0.25 : 2.0 / 3.0));
-    residual2_kernel<P><<<grid_res, NT_RES, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, nullptr, nullptr, Geo{},
-                                                         nullptr, StageCombine{}, 0, s, (s % R) + 1, ST_RUN, nxt, ca, cb);
+    residual2_batched<P><<<grid_res, NT_RES, smem, st>>>(in, g.pref(WK_RES), tot + WK_RES, ninst, s, (s % R) + 1,
+                                                          ST_RUN, nxt, ca, cb);
   }
   ctl_batched<<<1, 256, 0, st>>>(in, ninst, CTL_STEP_END, R, 0);
 }

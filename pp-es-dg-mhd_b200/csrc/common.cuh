@@ -250,6 +250,21 @@ __device__ __forceinline__ double ent_of(double rho, double prs, double gamma) {
   return -(rho * (log(prs) - gamma * log(rho)) / (gamma - 1.0));
 }
 
+// Exactly rounded arithmetic for the residual's flux functions: every product, sum and fused
+// multiply-add is written out, so the compiler has no freedom to contract or re-use products
+// differently in different kernels, and every kernel that inlines these functions (single
+// instance, re-try, batched, allocation-free) rounds them the same way.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+// a*a + b*b + c*c, left to right with fused multiply-adds
+__device__ __forceinline__ double dsq3(double a, double b, double c) { return dfma(c, c, dfma(b, b, dmul(a, a))); }
+// a1*b1 + a2*b2 + a3*b3, likewise
+__device__ __forceinline__ double ddot3(double a1, double b1, double a2, double b2, double a3, double b3) {
+  return dfma(a3, b3, dfma(a2, b2, dmul(a1, b1)));
+}
+
 // Entropy-conservative two-point flux, x (DIR=0, DG_solver.f90:1570-1609) or y (DIR=1,
 // DG_solver.f90:1611-1650).  a, b = (rho, vx, vy, vz, bx, by, bz, beta).
 //
@@ -267,184 +282,171 @@ __device__ __forceinline__ double ent_of(double rho, double prs, double gamma) {
 // igm1 = 1/(gamma-1), formed once by the caller.  Results agree with the reference's
 // expression order to a few ulp; the series/log branch is decided on the same u (to an ulp).
 __device__ __forceinline__ double series_divisor(double u) {
-  return 1.0 + u * (1.0 / 3.0 + u * (1.0 / 5.0 + u * (1.0 / 7.0)));
+  return dfma(u, dfma(u, dfma(u, 1.0 / 7.0, 1.0 / 5.0), 1.0 / 3.0), 1.0);
 }
 // 1 / series_divisor(u) by its own series, 1 - u/3 - 4u^2/45 - 44u^3/945 + 1147u^4/14175 (the
 // inverse of the power series; the truncation error is below 3e-22 relative for u < 1.4e-4),
 // so that the logarithmic mean of the common smooth case takes no division
 __device__ __forceinline__ double inv_series_divisor(double u) {
-  return 1.0 + u * (-1.0 / 3.0 + u * (-4.0 / 45.0 + u * (-44.0 / 945.0 + u * (1147.0 / 14175.0))));
+  return dfma(u, dfma(u, dfma(u, dfma(u, 1147.0 / 14175.0, -44.0 / 945.0), -4.0 / 45.0), -1.0 / 3.0), 1.0);
 }
 
 template <int DIR>
 __device__ __forceinline__ void ec_flux(const double* a, const double* b, double igm1, double* f) {
-  const double rho_s = a[0] + b[0], beta_s = a[7] + b[7];
-  const double rho_bar = 0.5 * rho_s;
-  const double vx_bar = 0.5 * (a[1] + b[1]);
-  const double vy_bar = 0.5 * (a[2] + b[2]);
-  const double vz_bar = 0.5 * (a[3] + b[3]);
-  const double bx_bar = 0.5 * (a[4] + b[4]);
-  const double by_bar = 0.5 * (a[5] + b[5]);
-  const double bz_bar = 0.5 * (a[6] + b[6]);
-  const double v_sq_bar = 0.5 * ((a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) + (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]));
-  const double b_sq_bar = 0.5 * ((a[4] * a[4] + a[5] * a[5] + a[6] * a[6]) + (b[4] * b[4] + b[5] * b[5] + b[6] * b[6]));
-  const double bvx = 0.5 * (a[7] * a[1] + b[7] * b[1]);
-  const double bvy = 0.5 * (a[7] * a[2] + b[7] * b[2]);
-  const double bvz = 0.5 * (a[7] * a[3] + b[7] * b[3]);
-  const double rho_d = a[0] - b[0], beta_d = a[7] - b[7];
+  const double rho_s = dadd(a[0], b[0]), beta_s = dadd(a[7], b[7]);
+  const double rho_bar = dmul(0.5, rho_s);
+  const double vx_bar = dmul(0.5, dadd(a[1], b[1]));
+  const double vy_bar = dmul(0.5, dadd(a[2], b[2]));
+  const double vz_bar = dmul(0.5, dadd(a[3], b[3]));
+  const double bx_bar = dmul(0.5, dadd(a[4], b[4]));
+  const double by_bar = dmul(0.5, dadd(a[5], b[5]));
+  const double bz_bar = dmul(0.5, dadd(a[6], b[6]));
+  const double v_sq_bar = dmul(0.5, dadd(dsq3(a[1], a[2], a[3]), dsq3(b[1], b[2], b[3])));
+  const double b_sq_bar = dmul(0.5, dadd(dsq3(a[4], a[5], a[6]), dsq3(b[4], b[5], b[6])));
+  const double bvx = dmul(0.5, dfma(b[7], b[1], dmul(a[7], a[1])));
+  const double bvy = dmul(0.5, dfma(b[7], b[2], dmul(a[7], a[2])));
+  const double bvz = dmul(0.5, dfma(b[7], b[3], dmul(a[7], a[3])));
+  const double rho_d = dsub(a[0], b[0]), beta_d = dsub(a[7], b[7]);
   // 1/rho_s and 1/beta_s from one reciprocal
-  const double r_rb = 1.0 / (rho_s * beta_s);
-  const double inv_bb = 2.0 * (rho_s * r_rb);  // 1 / beta_bar
-  const double fr = rho_d * (beta_s * r_rb), ur = fr * fr;
-  const double fb = beta_d * (0.5 * inv_bb), ub = fb * fb;
+  const double r_rb = 1.0 / dmul(rho_s, beta_s);
+  const double inv_bb = dmul(2.0, dmul(rho_s, r_rb));  // 1 / beta_bar
+  const double fr = dmul(rho_d, dmul(beta_s, r_rb)), ur = dmul(fr, fr);
+  const double fb = dmul(beta_d, dmul(0.5, inv_bb)), ub = dmul(fb, fb);
   // logarithmic mean of rho and divisor of that of beta: the series forms, replaced by the
   // logarithmic forms in the uncommon case
-  double rho_hat = rho_bar * inv_series_divisor(ur);
+  double rho_hat = dmul(rho_bar, inv_series_divisor(ur));
   double ffb = series_divisor(ub);
   if (ur >= 1.4e-4 || ub >= 1.4e-4) {
     if (ur >= 1.4e-4) rho_hat = rho_d / log(a[0] / b[0]);
-    if (ub >= 1.4e-4) ffb = 0.5 * log(a[7] / b[7]) / fb;
+    if (ub >= 1.4e-4) ffb = dmul(0.5, log(a[7] / b[7])) / fb;
   }
-  const double ptot = 0.5 * (b_sq_bar + rho_bar * inv_bb);
-  const double ecoef = 0.5 * (ffb * inv_bb * igm1 - v_sq_bar);
-  const double vb = vx_bar * bx_bar + vy_bar * by_bar + vz_bar * bz_bar;
+  const double ptot = dmul(0.5, dfma(rho_bar, inv_bb, b_sq_bar));
+  const double ecoef = dmul(0.5, dfma(dmul(ffb, inv_bb), igm1, -v_sq_bar));
+  const double vb = ddot3(vx_bar, bx_bar, vy_bar, by_bar, vz_bar, bz_bar);
+  const double bn = DIR == 0 ? bx_bar : by_bar;  // the field component normal to the flux direction
+  const double vn = DIR == 0 ? vx_bar : vy_bar;
+  f[0] = dmul(rho_hat, vn);
+  f[1] = dfma(vx_bar, f[0], -dmul(bn, bx_bar));
+  f[2] = dfma(vy_bar, f[0], -dmul(bn, by_bar));
+  f[3] = dfma(vz_bar, f[0], -dmul(bn, bz_bar));
   if (DIR == 0) {
-    f[0] = rho_hat * vx_bar;
-    f[1] = vx_bar * f[0] - bx_bar * bx_bar + ptot;
-    f[2] = vy_bar * f[0] - bx_bar * by_bar;
-    f[3] = vz_bar * f[0] - bx_bar * bz_bar;
+    f[1] = dadd(f[1], ptot);
     f[4] = 0.0;
-    f[5] = (bvx * by_bar - bvy * bx_bar) * inv_bb;
-    f[6] = (bvx * bz_bar - bvz * bx_bar) * inv_bb;
-    f[7] = ecoef * f[0] + (vx_bar * f[1] + vy_bar * f[2] + vz_bar * f[3]) +
-           (bx_bar * f[4] + by_bar * f[5] + bz_bar * f[6]) - 0.5 * vx_bar * b_sq_bar + vb * bx_bar;
+    f[5] = dmul(dfma(bvx, by_bar, -dmul(bvy, bx_bar)), inv_bb);
+    f[6] = dmul(dfma(bvx, bz_bar, -dmul(bvz, bx_bar)), inv_bb);
   } else {
-    f[0] = rho_hat * vy_bar;
-    f[1] = vx_bar * f[0] - by_bar * bx_bar;
-    f[2] = vy_bar * f[0] - by_bar * by_bar + ptot;
-    f[3] = vz_bar * f[0] - by_bar * bz_bar;
-    f[4] = (bvy * bx_bar - bvx * by_bar) * inv_bb;
+    f[2] = dadd(f[2], ptot);
+    f[4] = dmul(dfma(bvy, bx_bar, -dmul(bvx, by_bar)), inv_bb);
     f[5] = 0.0;
-    f[6] = (bvy * bz_bar - bvz * by_bar) * inv_bb;
-    f[7] = ecoef * f[0] + (vx_bar * f[1] + vy_bar * f[2] + vz_bar * f[3]) +
-           (bx_bar * f[4] + by_bar * f[5] + bz_bar * f[6]) - 0.5 * vy_bar * b_sq_bar + vb * by_bar;
+    f[6] = dmul(dfma(bvy, bz_bar, -dmul(bvz, by_bar)), inv_bb);
   }
+  // ecoef f0 + (v . f[1..3]) + (b . f[4..6]) - 0.5 vn |b|^2 + (v . b) bn
+  double e = dfma(ecoef, f[0], ddot3(vx_bar, f[1], vy_bar, f[2], vz_bar, f[3]));
+  e = dadd(e, dfma(bz_bar, f[6], dfma(by_bar, f[5], dmul(bx_bar, f[4]))));
+  e = dfma(dmul(-0.5, vn), b_sq_bar, e);
+  f[7] = dfma(vb, bn, e);
 }
 
 // ESPP_HLL_flux_x (DG_solver.f90:894-1071).  wl, wr: conserved states already rotated into the
 // face normal frame (swap_xy for y faces).  out[0..7] = numerical flux, out[8] = nBn,
 // out[9] = sl, out[10] = sr.  igm1 = 1/(gamma-1).  Quotients are formed as products with shared
-// reciprocals: 1/rho_l and 1/rho_r from 1/(rho_l rho_r); 1/p_l, 1/p_r and the Roe weight
-// 1/(sqrt(rho_l)+sqrt(rho_r)) from 1/((sqrt(rho_l)+sqrt(rho_r)) p_l p_r); 1/a_form; 1/(sr-sl).
-// The values agree with the reference's expression order to a few ulp.
+// reciprocals: 1/rho_l and 1/rho_r from 1/(rho_l rho_r); 1/p_l and 1/p_r from 1/(p_l p_r); the Roe
+// weight 1/(sqrt(rho_l)+sqrt(rho_r)); 1/a_form; 1/(sr-sl).  The values agree with the reference's
+// expression order to a few ulp.
 __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, double gamma, double igm1, double* out) {
   const double rho_l = wl[0], mx_l = wl[1], my_l = wl[2], mz_l = wl[3], bx_l = wl[4], by_l = wl[5], bz_l = wl[6], e_l = wl[7];
   const double rho_r = wr[0], mx_r = wr[1], my_r = wr[2], mz_r = wr[3], bx_r = wr[4], by_r = wr[5], bz_r = wr[6], e_r = wr[7];
-  const double gm1 = gamma - 1.0;
-  const double r_rho = 1.0 / (rho_l * rho_r);
-  const double ir_l = rho_r * r_rho, ir_r = rho_l * r_rho;
-  const double vx_l = ir_l * mx_l, vx_r = ir_r * mx_r;
-  const double vy_l = ir_l * my_l, vy_r = ir_r * my_r;
-  const double vz_l = ir_l * mz_l, vz_r = ir_r * mz_r;
-  const double ek_l = 0.5 * ir_l * (mx_l * mx_l + my_l * my_l + mz_l * mz_l);
-  const double ek_r = 0.5 * ir_r * (mx_r * mx_r + my_r * my_r + mz_r * mz_r);
-  const double bsq_l = bx_l * bx_l + by_l * by_l + bz_l * bz_l;
-  const double bsq_r = bx_r * bx_r + by_r * by_r + bz_r * bz_r;
-  const double pm_l = 0.5 * bsq_l, pm_r = 0.5 * bsq_r;
-  const double p_l = fmax(gm1 * (e_l - (ek_l + pm_l)), PP_EPS);
-  const double p_r = fmax(gm1 * (e_r - (ek_r + pm_r)), PP_EPS);
-  const double r_p = 1.0 / (p_l * p_r);
-  const double ip_l = p_r * r_p, ip_r = p_l * r_p;
-  const double pt_l = p_l + pm_l, pt_r = p_r + pm_r;
-  const double bu_l = bx_l * vx_l + by_l * vy_l + bz_l * vz_l;
-  const double bu_r = bx_r * vx_r + by_r * vy_r + bz_r * vz_r;
-  const double cs_l = gamma * p_l * ir_l, cs_r = gamma * p_r * ir_r;
-  const double ss_l = cs_l + bsq_l * ir_l, ss_r = cs_r + bsq_r * ir_r;
-  const double cf_l = sqrt(0.5 * (ss_l + sqrt(fmax(ss_l * ss_l - 4.0 * cs_l * ir_l * (bx_l * bx_l), 0.0))));
-  const double cf_r = sqrt(0.5 * (ss_r + sqrt(fmax(ss_r * ss_r - 4.0 * cs_r * ir_r * (bx_r * bx_r), 0.0))));
-  const double ith_l = rho_l * ip_l, ith_r = rho_r * ip_r;
-  const double phi_l = ith_l * bu_l, phi_r = ith_r * bu_r;
-  const double se_l = log(p_l) - gamma * log(rho_l);
-  const double se_r = log(p_r) - gamma * log(rho_r);
-  const double ef_l = (-rho_l * se_l * igm1) * vx_l;
-  const double ef_r = (-rho_r * se_r * igm1) * vx_r;
+  const double gm1 = dsub(gamma, 1.0);
+  const double r_rho = 1.0 / dmul(rho_l, rho_r);
+  const double ir_l = dmul(rho_r, r_rho), ir_r = dmul(rho_l, r_rho);
+  const double vx_l = dmul(ir_l, mx_l), vx_r = dmul(ir_r, mx_r);
+  const double vy_l = dmul(ir_l, my_l), vy_r = dmul(ir_r, my_r);
+  const double vz_l = dmul(ir_l, mz_l), vz_r = dmul(ir_r, mz_r);
+  const double ek_l = dmul(dmul(0.5, ir_l), dsq3(mx_l, my_l, mz_l));
+  const double ek_r = dmul(dmul(0.5, ir_r), dsq3(mx_r, my_r, mz_r));
+  const double bsq_l = dsq3(bx_l, by_l, bz_l);
+  const double bsq_r = dsq3(bx_r, by_r, bz_r);
+  const double pm_l = dmul(0.5, bsq_l), pm_r = dmul(0.5, bsq_r);
+  const double p_l = fmax(dmul(gm1, dsub(e_l, dadd(ek_l, pm_l))), PP_EPS);
+  const double p_r = fmax(dmul(gm1, dsub(e_r, dadd(ek_r, pm_r))), PP_EPS);
+  const double r_p = 1.0 / dmul(p_l, p_r);
+  const double ip_l = dmul(p_r, r_p), ip_r = dmul(p_l, r_p);
+  const double pt_l = dadd(p_l, pm_l), pt_r = dadd(p_r, pm_r);
+  const double bu_l = ddot3(bx_l, vx_l, by_l, vy_l, bz_l, vz_l);
+  const double bu_r = ddot3(bx_r, vx_r, by_r, vy_r, bz_r, vz_r);
+  const double cs_l = dmul(dmul(gamma, p_l), ir_l), cs_r = dmul(dmul(gamma, p_r), ir_r);
+  const double ss_l = dfma(bsq_l, ir_l, cs_l), ss_r = dfma(bsq_r, ir_r, cs_r);
+  const double cf_l = sqrt(dmul(0.5, dadd(ss_l, sqrt(fmax(dfma(ss_l, ss_l, -dmul(dmul(dmul(4.0, cs_l), ir_l), dmul(bx_l, bx_l))), 0.0)))));
+  const double cf_r = sqrt(dmul(0.5, dadd(ss_r, sqrt(fmax(dfma(ss_r, ss_r, -dmul(dmul(dmul(4.0, cs_r), ir_r), dmul(bx_r, bx_r))), 0.0)))));
+  const double ith_l = dmul(rho_l, ip_l), ith_r = dmul(rho_r, ip_r);
+  const double phi_l = dmul(ith_l, bu_l), phi_r = dmul(ith_r, bu_r);
+  const double se_l = dfma(-gamma, log(rho_l), log(p_l));
+  const double se_r = dfma(-gamma, log(rho_r), log(p_r));
+  const double ef_l = dmul(dmul(dmul(-rho_l, se_l), igm1), vx_l);
+  const double ef_r = dmul(dmul(dmul(-rho_r, se_r), igm1), vx_r);
   double fl[8], fr[8], vl[8], vr[8];
   fl[0] = mx_l;
-  fl[1] = vx_l * mx_l - bx_l * bx_l + pt_l;
-  fl[2] = vx_l * my_l - by_l * bx_l;
-  fl[3] = vx_l * mz_l - bz_l * bx_l;
+  fl[1] = dadd(dfma(vx_l, mx_l, -dmul(bx_l, bx_l)), pt_l);
+  fl[2] = dfma(vx_l, my_l, -dmul(by_l, bx_l));
+  fl[3] = dfma(vx_l, mz_l, -dmul(bz_l, bx_l));
   fl[4] = 0.0;
-  fl[5] = -(bx_l * vy_l - by_l * vx_l);
-  fl[6] = bz_l * vx_l - bx_l * vz_l;
-  fl[7] = vx_l * (e_l + pt_l) - bx_l * bu_l;
+  fl[5] = -dfma(bx_l, vy_l, -dmul(by_l, vx_l));
+  fl[6] = dfma(bz_l, vx_l, -dmul(bx_l, vz_l));
+  fl[7] = dfma(vx_l, dadd(e_l, pt_l), -dmul(bx_l, bu_l));
   fr[0] = mx_r;
-  fr[1] = vx_r * mx_r - bx_r * bx_r + pt_r;
-  fr[2] = vx_r * my_r - by_r * bx_r;
-  fr[3] = vx_r * mz_r - bz_r * bx_r;
+  fr[1] = dadd(dfma(vx_r, mx_r, -dmul(bx_r, bx_r)), pt_r);
+  fr[2] = dfma(vx_r, my_r, -dmul(by_r, bx_r));
+  fr[3] = dfma(vx_r, mz_r, -dmul(bz_r, bx_r));
   fr[4] = 0.0;
-  fr[5] = -(bx_r * vy_r - by_r * vx_r);
-  fr[6] = bz_r * vx_r - bx_r * vz_r;
-  fr[7] = vx_r * (e_r + pt_r) - bx_r * bu_r;
-  vl[0] = (gamma - se_l) * igm1 - ek_l * ip_l;
-  vl[1] = mx_l * ip_l;
-  vl[2] = my_l * ip_l;
-  vl[3] = mz_l * ip_l;
-  vl[4] = ith_l * bx_l;
-  vl[5] = ith_l * by_l;
-  vl[6] = ith_l * bz_l;
+  fr[5] = -dfma(bx_r, vy_r, -dmul(by_r, vx_r));
+  fr[6] = dfma(bz_r, vx_r, -dmul(bx_r, vz_r));
+  fr[7] = dfma(vx_r, dadd(e_r, pt_r), -dmul(bx_r, bu_r));
+  vl[0] = dfma(-ek_l, ip_l, dmul(dsub(gamma, se_l), igm1));
+  vl[1] = dmul(mx_l, ip_l);
+  vl[2] = dmul(my_l, ip_l);
+  vl[3] = dmul(mz_l, ip_l);
+  vl[4] = dmul(ith_l, bx_l);
+  vl[5] = dmul(ith_l, by_l);
+  vl[6] = dmul(ith_l, bz_l);
   vl[7] = -ith_l;
-  vr[0] = (gamma - se_r) * igm1 - ek_r * ip_r;
-  vr[1] = mx_r * ip_r;
-  vr[2] = my_r * ip_r;
-  vr[3] = mz_r * ip_r;
-  vr[4] = ith_r * bx_r;
-  vr[5] = ith_r * by_r;
-  vr[6] = ith_r * bz_r;
+  vr[0] = dfma(-ek_r, ip_r, dmul(dsub(gamma, se_r), igm1));
+  vr[1] = dmul(mx_r, ip_r);
+  vr[2] = dmul(my_r, ip_r);
+  vr[3] = dmul(mz_r, ip_r);
+  vr[4] = dmul(ith_r, bx_r);
+  vr[5] = dmul(ith_r, by_r);
+  vr[6] = dmul(ith_r, bz_r);
   vr[7] = -ith_r;
   const double sq_l = sqrt(rho_l), sq_r = sqrt(rho_r);
-  const double isum = 1.0 / (sq_l + sq_r);
-  const double vx_roe = (vx_l * sq_l + vx_r * sq_r) * isum;
-  const double db = sqrt((bx_l - bx_r) * (bx_l - bx_r) + (by_l - by_r) * (by_l - by_r) + (bz_l - bz_r) * (bz_l - bz_r)) * isum;
-  const double sl_pp = fmin(vx_l, vx_roe) - cf_l - db;
-  const double sr_pp = fmax(vx_r, vx_roe) + cf_r + db;
+  const double isum = 1.0 / dadd(sq_l, sq_r);
+  const double vx_roe = dmul(dfma(vx_r, sq_r, dmul(vx_l, sq_l)), isum);
+  const double db = dmul(sqrt(dsq3(dsub(bx_l, bx_r), dsub(by_l, by_r), dsub(bz_l, bz_r))), isum);
+  const double sl_pp = dsub(dsub(fmin(vx_l, vx_roe), cf_l), db);
+  const double sr_pp = dadd(dadd(fmax(vx_r, vx_roe), cf_r), db);
   double da = 0.0, dbl = 0.0, dbr = 0.0;
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    const double dfs = fr[s] - fl[s];
-    da += (vr[s] - vl[s]) * (wr[s] - wl[s]);
-    dbl += vl[s] * dfs;
-    dbr += vr[s] * dfs;
+    const double dfs = dsub(fr[s], fl[s]);
+    da = dfma(dsub(vr[s], vl[s]), dsub(wr[s], wl[s]), da);
+    dbl = dfma(vl[s], dfs, dbl);
+    dbr = dfma(vr[s], dfs, dbr);
   }
-  const double ia = 1.0 / (fmax(da, 0.0) + 1e-8);
-  const double bl_form = (ef_r - ef_l) - dbl - phi_l * (bx_r - bx_l);
-  const double br_form = (ef_r - ef_l) - dbr - phi_r * (bx_r - bx_l);
-  const double al = fmax(bl_form * ia, 0.0);
-  const double ar = fmax(br_form * ia, 0.0);
-  const double aa = sqrt(al * ar);
-  const double sl = fmin(fmin(-(ar + aa), sl_pp), 0.0);
-  const double sr = fmax(fmax(al + aa, sr_pp), 0.0);
-  const double idsl = 1.0 / (sr - sl);
-  const double wl_ = sr * idsl, wr_ = -sl * idsl, wd = (sl * sr) * idsl;
+  const double ia = 1.0 / dadd(fmax(da, 0.0), 1e-8);
+  const double def = dsub(ef_r, ef_l), jbx = dsub(bx_r, bx_l);
+  const double bl_form = dfma(-phi_l, jbx, dsub(def, dbl));
+  const double br_form = dfma(-phi_r, jbx, dsub(def, dbr));
+  const double al = fmax(dmul(bl_form, ia), 0.0);
+  const double ar = fmax(dmul(br_form, ia), 0.0);
+  const double aa = sqrt(dmul(al, ar));
+  const double sl = fmin(fmin(-dadd(ar, aa), sl_pp), 0.0);
+  const double sr = fmax(fmax(dadd(al, aa), sr_pp), 0.0);
+  const double idsl = 1.0 / dsub(sr, sl);
+  const double wl_ = dmul(sr, idsl), wr_ = dmul(-sl, idsl), wd = dmul(dmul(sl, sr), idsl);
 #pragma unroll
-  for (int s = 0; s < 8; ++s) out[s] = wl_ * fl[s] + wr_ * fr[s] + wd * (wr[s] - wl[s]);
-  out[8] = wl_ * bx_l + wr_ * bx_r;
+  for (int s = 0; s < 8; ++s) out[s] = dfma(wd, dsub(wr[s], wl[s]), dfma(wr_, fr[s], dmul(wl_, fl[s])));
+  out[8] = dfma(wr_, bx_r, dmul(wl_, bx_l));
   out[9] = sl;
   out[10] = sr;
-}
-
-// max fast magnetosonic speed of a node in x and y (DG_solver.f90:749-770)
-__device__ __forceinline__ void node_sigma(const double* w, double gamma, double& sx, double& sy) {
-  const double rho = w[0];
-  const double ir = 1.0 / rho;
-  const double vx = ir * w[1], vy = ir * w[2];
-  const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
-  const double bsq = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
-  const double pf = fmax((gamma - 1.0) * (w[7] - (ek + 0.5 * bsq)), PP_EPS);
-  const double cs = gamma * pf * ir;
-  const double ss = cs + bsq * ir;
-  const double coef = 4.0 * cs * ir;
-  sx = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
-  sy = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
 }
 
 }  // namespace mhd

@@ -169,6 +169,12 @@ int init_device_tables(int dev) {
   CK(cudaFuncSetAttribute(residual2_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<1>::BYTES));
   CK(cudaFuncSetAttribute(residual2_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<2>::BYTES));
   CK(cudaFuncSetAttribute(residual2_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_batched<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_batched<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_batched<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<3>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_persistent<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<1>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_persistent<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<2>::BYTES));
+  CK(cudaFuncSetAttribute(residual2_persistent<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Res2Layout<3>::BYTES));
   g_dev_init[dev] = true;
   return MHD_OK;
 }
@@ -213,9 +219,8 @@ void launch_bc(mhd_gpu* h, double* u, int gate) {
 template <int P>
 void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate, StageCombine sc = StageCombine{}) {
   using L = Res2Layout<P>;
-  const int ntiles = ((h->nx + L::TX - 1) / L::TX) * ((h->ny + L::TY - 1) / L::TY);
-  residual2_kernel<P><<<ntiles, L::NT, L::BYTES, h->stream>>>(nullptr, nullptr, nullptr, nullptr, u, ut, h->geo,
-                                                              h->ctrl, sc, ntiles, 0, 0, gate, 0, 0.0, 0.0);
+  dim3 grid((h->nx + L::TX - 1) / L::TX, (h->ny + L::TY - 1) / L::TY);
+  residual2_kernel<P><<<grid, L::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate, sc);
 }
 
 // the re-try residual of a try (gate ST_RECOMPUTE, usually closed): a persistent grid of the CTAs
@@ -227,7 +232,7 @@ int res_resident_ctas(int dev) {
   if (!cached[dev]) {
     int nsm = 0, per_sm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, residual2_kernel<P>, Res2Layout<P>::NT,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, residual2_persistent<P>, Res2Layout<P>::NT,
                                                   Res2Layout<P>::BYTES);
     cached[dev] = std::max(1, nsm) * std::max(1, per_sm);
   }
@@ -237,8 +242,8 @@ template <int P>
 void launch_residual_retry(mhd_gpu* h, const double* u, double* ut) {
   using L = Res2Layout<P>;
   const int ntx = (h->nx + L::TX - 1) / L::TX, ntiles = ntx * ((h->ny + L::TY - 1) / L::TY);
-  residual2_kernel<P><<<std::min(ntiles, res_resident_ctas<P>(h->device)), L::NT, L::BYTES, h->stream>>>(
-      nullptr, nullptr, nullptr, nullptr, u, ut, h->geo, h->ctrl, StageCombine{}, ntiles, 0, 0, ST_RECOMPUTE, 0, 0.0, 0.0);
+  residual2_persistent<P><<<std::min(ntiles, res_resident_ctas<P>(h->device)), L::NT, L::BYTES, h->stream>>>(
+      u, ut, h->geo, h->ctrl, ST_RECOMPUTE, ntx, ntiles);
 }
 
 template <int P>
@@ -1104,23 +1109,17 @@ extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, 
   switch (p) {
     case 1: {
       using L = Res2Layout<1>;
-      const int nt = ((nx + L::TX - 1) / L::TX) * ((ny + L::TY - 1) / L::TY);
-      residual2_kernel<1><<<nt, L::NT, L::BYTES, s>>>(nullptr, nullptr, nullptr, nullptr, u, ut, g, ctrl, StageCombine{},
-                                                       nt, 0, 0, GATE_ALWAYS, 0, 0.0, 0.0);
+      residual2_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     case 2: {
       using L = Res2Layout<2>;
-      const int nt = ((nx + L::TX - 1) / L::TX) * ((ny + L::TY - 1) / L::TY);
-      residual2_kernel<2><<<nt, L::NT, L::BYTES, s>>>(nullptr, nullptr, nullptr, nullptr, u, ut, g, ctrl, StageCombine{},
-                                                       nt, 0, 0, GATE_ALWAYS, 0, 0.0, 0.0);
+      residual2_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     default: {
       using L = Res2Layout<3>;
-      const int nt = ((nx + L::TX - 1) / L::TX) * ((ny + L::TY - 1) / L::TY);
-      residual2_kernel<3><<<nt, L::NT, L::BYTES, s>>>(nullptr, nullptr, nullptr, nullptr, u, ut, g, ctrl, StageCombine{},
-                                                       nt, 0, 0, GATE_ALWAYS, 0, 0.0, 0.0);
+      residual2_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
   }

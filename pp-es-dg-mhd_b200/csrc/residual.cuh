@@ -273,13 +273,14 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
 #pragma unroll
     for (int v = 0; v < 8; ++v) w[v] = cw[v * NN];
   }
+  // (all arithmetic of the tile is exactly rounded as written: dmul/dadd/dsub/dfma of common.cuh)
   const double ir = 1.0 / w[0];
-  const double vx = ir * w[1], vy = ir * w[2], vz = ir * w[3];
+  const double vx = dmul(ir, w[1]), vy = dmul(ir, w[2]), vz = dmul(ir, w[3]);
   double pt, sgx, sgy, pp[8];  // pp: (rho, vx, vy, vz, Bx, By, Bz, beta), the EC flux's inputs
   {
-    const double ek = 0.5 * ir * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
-    const double bsq = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
-    const double pf = fmax((gamma - 1.0) * (w[7] - (ek + 0.5 * bsq)), PP_EPS);
+    const double ek = dmul(dmul(0.5, ir), dsq3(w[1], w[2], w[3]));
+    const double bsq = dsq3(w[4], w[5], w[6]);
+    const double pf = fmax(dmul(dsub(gamma, 1.0), dsub(w[7], dfma(0.5, bsq, ek))), PP_EPS);
     pp[0] = w[0];
     pp[1] = vx;
     pp[2] = vy;
@@ -287,11 +288,11 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
     pp[4] = w[4];
     pp[5] = w[5];
     pp[6] = w[6];
-    pp[7] = 0.5 * w[0] / pf;
-    const double cs = gamma * pf * ir, ss = cs + bsq * ir, coef = 4.0 * cs * ir;
-    pt = pf + 0.5 * bsq;
-    sgx = fabs(vx) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[4] * w[4]), 0.0)), 0.0));
-    sgy = fabs(vy) + sqrt(0.5 * fmax(ss + sqrt(fmax(ss * ss - coef * (w[5] * w[5]), 0.0)), 0.0));
+    pp[7] = dmul(0.5, w[0]) / pf;
+    const double cs = dmul(dmul(gamma, pf), ir), ss = dfma(bsq, ir, cs), coef = dmul(dmul(4.0, cs), ir);
+    pt = dfma(0.5, bsq, pf);
+    sgx = dadd(fabs(vx), sqrt(dmul(0.5, fmax(dadd(ss, sqrt(fmax(dfma(ss, ss, -dmul(coef, dmul(w[4], w[4]))), 0.0))), 0.0))));
+    sgy = dadd(fabs(vy), sqrt(dmul(0.5, fmax(dadd(ss, sqrt(fmax(dfma(ss, ss, -dmul(coef, dmul(w[5], w[5]))), 0.0))), 0.0))));
   }
   auto Dm = [&](int i) { return s_dm[i]; };
   // the partner lane of node (kk, ll) of this lane's element
@@ -309,24 +310,24 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   // (DG_solver.f90:833), with the diagonal and Godunov-Powell terms
   auto node_fluxes = [&](double* F, double* Gf, double* GP) {
     const double bx = w[4], by = w[5], bz = w[6];
-    const double bu = bx * vx + by * vy + bz * vz;
-    const double ex = by * vz - bz * vy, ey = bz * vx - bx * vz, ez = bx * vy - by * vx;
+    const double bu = ddot3(bx, vx, by, vy, bz, vz);
+    const double ex = dfma(by, vz, -dmul(bz, vy)), ey = dfma(bz, vx, -dmul(bx, vz)), ez = dfma(bx, vy, -dmul(by, vx));
     F[0] = w[1];
-    F[1] = vx * w[1] - bx * bx + pt;
-    F[2] = vx * w[2] - by * bx;
-    F[3] = vx * w[3] - bz * bx;
+    F[1] = dadd(dfma(vx, w[1], -dmul(bx, bx)), pt);
+    F[2] = dfma(vx, w[2], -dmul(by, bx));
+    F[3] = dfma(vx, w[3], -dmul(bz, bx));
     F[4] = 0.0;
     F[5] = -ez;
     F[6] = ey;
-    F[7] = vx * (w[7] + pt) - bx * bu;
+    F[7] = dfma(vx, dadd(w[7], pt), -dmul(bx, bu));
     Gf[0] = w[2];
-    Gf[1] = vy * w[1] - bx * by;
-    Gf[2] = vy * w[2] - by * by + pt;
-    Gf[3] = vy * w[3] - bz * by;
+    Gf[1] = dfma(vy, w[1], -dmul(bx, by));
+    Gf[2] = dadd(dfma(vy, w[2], -dmul(by, by)), pt);
+    Gf[3] = dfma(vy, w[3], -dmul(bz, by));
     Gf[4] = ez;
     Gf[5] = 0.0;
     Gf[6] = -ex;
-    Gf[7] = vy * (w[7] + pt) - by * bu;
+    Gf[7] = dfma(vy, dadd(w[7], pt), -dmul(by, bu));
     GP[0] = 0.0;
     GP[1] = bx;
     GP[2] = by;
@@ -340,7 +341,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   {
     double F[8], Gf[8], GP[8];
     node_fluxes(F, Gf, GP);
-    const double divB = sxh * dbx + syh * dby;
+    const double divB = dfma(syh, dby, dmul(sxh, dbx));
     const double ckk = 2.0 * sxh * Dm(k + N * k), cll = 2.0 * syh * Dm(l + N * l);
 #pragma unroll
     for (int v = 0; v < 8; ++v) acc[v] = __fma_rn(-divB, GP[v], __fma_rn(-cll, Gf[v], -__dmul_rn(ckk, F[v])));
@@ -485,48 +486,56 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   return true;
 }
 
-// The residual kernel, for every use: a single instance (insts == nullptr; its pointers, geometry
-// and next-stage combination are the one_* arguments and it has one_items tiles) or the members of a
-// batch group (the device table insts / pref / nwork / ninst; the state is slot src, the result
-// goes to ut[dst], or (next_stage > 0) the combination of stage next_stage goes to slot
-// next_stage).  The CTAs take contiguous shares of the items (tiles, row-major per member): a grid
-// of one CTA per tile for a plain launch, a persistent grid of the resident CTAs for the usually
-// gated re-try launch and for batches.  There is one call of residual_tile2 in one kernel, so every
-// use runs the same compiled arithmetic: a batch member is bitwise equal to its solo run.
+// single instance: one CTA per tile
 template <int P>
 __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
-    residual2_kernel(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
-                     const int* __restrict__ nwork, const int* __restrict__ ninst, const double* one_u,
-                     double* one_ut, Geo one_g, Ctrl* one_ctrl, StageCombine one_sc, int one_items, int src,
-                     int dst, int gate, int next_stage, double ca, double cb) {
-  if (!insts && !gate_open(one_ctrl, gate)) return;
+    residual2_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
+                     StageCombine sc) {
+  if (!gate_open(ctrl, gate)) return;
   extern __shared__ __align__(16) double sm[];
   res2_prologue<P>(sm);
   unsigned phase = 0;
-  const int nw = insts ? *nwork : one_items, n = insts ? *ninst : 1;
-  for (BatchWalk it(insts ? pref : nullptr, n, nw); it.more(); it.next()) {
-    const double* u;
-    double* ut;
-    Geo g;
-    Ctrl* ctrl;
-    StageCombine sc{};
-    if (insts) {
-      const InstDesc& d = insts[it.m];
-      u = d.u[src];
-      ut = d.ut[dst];
-      g = d.g;
-      ctrl = d.ctrl;
-      if (next_stage > 0) sc = StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt};
-    } else {
-      u = one_u;
-      ut = one_ut;
-      g = one_g;
-      ctrl = one_ctrl;
-      sc = one_sc;
-    }
-    if (!gate_open(ctrl, gate)) continue;
-    const int ntx = (g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX, local = it.local();
-    if (!residual_tile2<P>(u, ut, g, ctrl, local % ntx, local / ntx, sm, phase, sc)) return;
+  residual_tile2<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, phase, sc);
+}
+
+// single instance, persistent: CTA b computes tiles b, b + gridDim.x, ... (row-major, ntx per row).
+// For a launch that is usually gated off (the re-try residual of every try): a grid of resident
+// CTAs that return at once costs far less than one CTA per tile.
+template <int P>
+__global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
+    residual2_persistent(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
+                         int ntx, int ntiles) {
+  if (!gate_open(ctrl, gate)) return;
+  extern __shared__ __align__(16) double sm[];
+  res2_prologue<P>(sm);
+  unsigned phase = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if (!residual_tile2<P>(u, ut, g, ctrl, t % ntx, t / ntx, sm, phase, StageCombine{})) return;
+    __syncthreads();  // the next tile reuses shared memory
+  }
+}
+
+// many instances of degree P: a persistent grid walks every member's tiles (row-major per member);
+// the state is slot `src`, the result goes to ut[dst], or (next_stage > 0) the combination of
+// stage next_stage goes to slot next_stage.  The tile's arithmetic is fully rounded as written
+// (explicit fused multiply-adds, see common.cuh), so a member is bitwise equal to its solo run
+// although this is a different kernel.
+template <int P>
+__global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
+    residual2_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
+                      const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate,
+                      int next_stage, double ca, double cb) {
+  extern __shared__ __align__(16) double sm[];
+  res2_prologue<P>(sm);
+  unsigned phase = 0;
+  const int nw = *nwork, n = *ninst;
+  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
+    const int m = it.m, local = it.local();
+    const InstDesc& d = insts[m];
+    if (!gate_open(d.ctrl, gate)) continue;
+    const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
+    const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
+    if (!residual_tile2<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc)) return;
     __syncthreads();  // the next tile reuses shared memory
   }
 }
