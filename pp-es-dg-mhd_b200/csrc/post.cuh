@@ -303,20 +303,40 @@ __device__ __forceinline__ double stage1_node(const Stage1Src& s1, const Geo& g,
   return neg ? -x : x;
 }
 
+// Row and column of element e of the ghosted grid (rows of nxg elements) by one 32-bit division
+// (the element count of any mesh that fits on the device is below 2^32; a 64-bit division by a
+// run-time divisor is a long software sequence), and a position advanced along the rows.
+struct GridRC {
+  int j, i;
+};
+__device__ __forceinline__ GridRC grid_rc(long long e, int nxg) {
+  const unsigned q = (unsigned)e / (unsigned)nxg;
+  return GridRC{(int)q, (int)((unsigned)e - q * (unsigned)nxg)};
+}
+__device__ __forceinline__ GridRC grid_adv(GridRC p, int d, int nxg) {  // d >= 0 elements further
+  p.i += d;
+  while (p.i >= nxg) {
+    p.i -= nxg;
+    ++p.j;
+  }
+  return p;
+}
+
 // Queues this warp's elements of `chunk` into its shared buffers as one cp.async group (16-byte
 // pieces; element blocks are multiples of 16 bytes): the blocks of u, or, with a stage-1 source,
 // the blocks of u_con (bu) and k1 (bk) of the interior elements (ghost elements are formed from
 // direct loads).  bu, bk: G * EB doubles each, 16-byte aligned.
 template <int P>
 __device__ __forceinline__ void pp_prefetch(const double* __restrict__ u, const Geo& g, long long chunk,
-                                            const Stage1Src& s1, double* bu, double* bk) {
+                                            GridRC cpos, const Stage1Src& s1, double* bu, double* bk) {
   using C = PPCfg<P>;
   constexpr int EB = C::EB, G = C::G, TE = C::TE, H2 = EB / 2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nx = g.nx, NXG = nx + 2;
   const long long total = (long long)NXG * (g.ny + 2);
-  const long long ef = chunk * TE + warp * G;  // the warp's first element
-  const int jf = (int)(ef / NXG), if_ = (int)(ef - (long long)jf * NXG);
+  const long long ef = chunk * TE + warp * G;  // the warp's first element (cpos: the chunk's first)
+  const GridRC fp = grid_adv(cpos, warp * G, NXG);
+  const int jf = fp.j, if_ = fp.i;
 #pragma unroll
   for (int it = lane; it < G * H2; it += 32) {
     const int k = it / H2, o = 2 * (it - k * H2);
@@ -341,13 +361,13 @@ __device__ __forceinline__ void pp_prefetch(const double* __restrict__ u, const 
 
 template <int P, bool NEEDG, bool PF>
 __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double* __restrict__ u_avg, const Geo& g,
-                                                 Ctrl* ctrl, long long chunk, int apply_ldf, int need_global,
+                                                 Ctrl* ctrl, long long chunk, GridRC cpos, int apply_ldf, int need_global,
                                                  int ent_offset, double* __restrict__ partial_out,  // 8 doubles
                                                  double* __restrict__ cell_ent_DG, double* __restrict__ cell_ent_FV,
                                                  unsigned char* __restrict__ cell_ent_nan, int limit,
                                                  const double* s_A, double* s_ldf, double* s_red, int* s_cnt,
                                                  const Stage1Src& s1,
-                                                 double* bu, double* bk, long long next_chunk) {
+                                                 double* bu, double* bk, long long next_chunk, GridRC npos) {
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -363,8 +383,9 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   bool valid = false, inner = false;
   int i = 0, j = 0;
   if (el < ne) {
-    j = (int)(e / NXG);
-    i = (int)(e - (long long)j * NXG);
+    const GridRC me = grid_adv(cpos, el, NXG);  // cpos: the chunk's first element
+    j = me.j;
+    i = me.i;
     const bool ii = (i >= 1 && i <= nx), jj = (j >= 1 && j <= ny);
     valid = ii || jj;  // DG_solver.f90:165 (corners are skipped)
     inner = ii && jj;
@@ -387,7 +408,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
       for (int v = 0; v < 8; ++v) x[v] = act ? pu[v * NN] : 0.0;
     }
     __syncwarp();  // every lane has read the buffers: queue the next chunk into them
-    if (next_chunk >= 0) pp_prefetch<P>(u, g, next_chunk, s1, bu, bk);
+    if (next_chunk >= 0) pp_prefetch<P>(u, g, next_chunk, npos, s1, bu, bk);
   } else if (s1.u0) {
     const double dts = __dmul_rn(s1.coef, *s1.dt);
 #pragma unroll
@@ -524,7 +545,12 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
   // the copies of a warp's next chunk are in flight while it works on this one
   double* bu = s_pf + (threadIdx.x >> 5) * 2 * C::G * C::EB;
   double* bk = bu + C::G * C::EB;
-  if (blockIdx.x < nchunks) pp_prefetch<P>(u, g, blockIdx.x, s1, bu, bk);
+  // grid positions of the chunks' first elements, advanced by the CTA's stride (no division in
+  // the loop)
+  const int NXG = g.nx + 2;
+  const GridRC stride = grid_rc((long long)gridDim.x * C::TE, NXG);
+  GridRC pos = grid_rc((long long)blockIdx.x * C::TE, NXG);
+  if (blockIdx.x < nchunks) pp_prefetch<P>(u, g, blockIdx.x, pos, s1, bu, bk);
   // the chunk sums of consecutive chunks go to alternate halves of s_red: the barrier of chunk
   // k + 1 orders the reads of chunk k before the writes of chunk k + 2
   int half = 0;
@@ -532,9 +558,15 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     cp_async_wait_all();
     __syncwarp();
     const long long nxt = c + gridDim.x < nchunks ? (long long)c + gridDim.x : -1;
-    pp_avg_ldf_chunk<P, NEEDG, true>(u, u_avg, g, ctrl, c, apply_ldf, need_global, ent_offset,
+    GridRC npos{pos.j + stride.j, pos.i + stride.i};
+    if (npos.i >= NXG) {
+      npos.i -= NXG;
+      ++npos.j;
+    }
+    pp_avg_ldf_chunk<P, NEEDG, true>(u, u_avg, g, ctrl, c, pos, apply_ldf, need_global, ent_offset,
                                      partial_sum + (long long)c * 8, cell_ent_DG, cell_ent_FV, cell_ent_nan, limit,
-                                     s_A, s_ldf, s_red + half * C::TE * 8, &s_cnt, s1, bu, bk, nxt);
+                                     s_A, s_ldf, s_red + half * C::TE * 8, &s_cnt, s1, bu, bk, nxt, npos);
+    pos = npos;
   }
   __syncthreads();
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
@@ -568,10 +600,11 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, FINAL ? (PPCfg<P>::MINB > 3 ? 3 
     __syncthreads();
     const int need_global = FINAL && d.use_oedg;
     const Stage1Src s1 = stage1 ? Stage1Src{d.u[0], d.ut[1], &d.ctrl->dt, stage1_coef(d.R)} : Stage1Src{};
-    pp_avg_ldf_chunk<P, FINAL, false>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk, d.use_ldf, need_global,
+    pp_avg_ldf_chunk<P, FINAL, false>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk,
+                                      grid_rc((long long)chunk * C::TE, d.g.nx + 2), d.use_ldf, need_global,
                                       d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
                                       d.cell_ent_nan, !FINAL, s_A, s_ldf, s_red, &s_cnt, s1,
-                                      nullptr, nullptr, -1);
+                                      nullptr, nullptr, -1, GridRC{0, 0});
     __syncthreads();
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }

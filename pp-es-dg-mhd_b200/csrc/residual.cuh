@@ -215,10 +215,12 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   }
 
   const double igm1 = 1.0 / (gamma - 1.0);
-  // ---- phase 1: interface fluxes, every face node of the tile once, spread evenly over warps ----
+  // ---- phase 1: interface fluxes, every face node of the tile once ----
+  // Thread-major: the items fill whole warps first, so the fewest warps run this code (a warp
+  // pays its issue slots whether or not all its lanes have an item); the others go on to phase 2.
   {
     constexpr int NH = L::NFX + L::NFY;
-    for (int f = warp + NW * lane; f < NH; f += NT) {
+    for (int f = tid; f < NH; f += NT) {
       const bool ydir = f >= L::NFX;
       const double *pl, *pr;
       int sl, sr;
