@@ -384,7 +384,7 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
   const double se_r = dfma(-gamma, log(rho_r), log(p_r));
   const double ef_l = dmul(dmul(dmul(-rho_l, se_l), igm1), vx_l);
   const double ef_r = dmul(dmul(dmul(-rho_r, se_r), igm1), vx_r);
-  double fl[8], fr[8], vl[8], vr[8];
+  double fl[8], fr[8];
   fl[0] = mx_l;
   fl[1] = dadd(dfma(vx_l, mx_l, -dmul(bx_l, bx_l)), pt_l);
   fl[2] = dfma(vx_l, my_l, -dmul(by_l, bx_l));
@@ -401,35 +401,34 @@ __device__ __forceinline__ void espp_hll(const double* wl, const double* wr, dou
   fr[5] = -dfma(bx_r, vy_r, -dmul(by_r, vx_r));
   fr[6] = dfma(bz_r, vx_r, -dmul(bx_r, vz_r));
   fr[7] = dfma(vx_r, dadd(e_r, pt_r), -dmul(bx_r, bu_r));
-  vl[0] = dfma(-ek_l, ip_l, dmul(dsub(gamma, se_l), igm1));
-  vl[1] = dmul(mx_l, ip_l);
-  vl[2] = dmul(my_l, ip_l);
-  vl[3] = dmul(mz_l, ip_l);
-  vl[4] = dmul(ith_l, bx_l);
-  vl[5] = dmul(ith_l, by_l);
-  vl[6] = dmul(ith_l, bz_l);
-  vl[7] = -ith_l;
-  vr[0] = dfma(-ek_r, ip_r, dmul(dsub(gamma, se_r), igm1));
-  vr[1] = dmul(mx_r, ip_r);
-  vr[2] = dmul(my_r, ip_r);
-  vr[3] = dmul(mz_r, ip_r);
-  vr[4] = dmul(ith_r, bx_r);
-  vr[5] = dmul(ith_r, by_r);
-  vr[6] = dmul(ith_r, bz_r);
-  vr[7] = -ith_r;
   const double sq_l = sqrt(rho_l), sq_r = sqrt(rho_r);
   const double isum = 1.0 / dadd(sq_l, sq_r);
   const double vx_roe = dmul(dfma(vx_r, sq_r, dmul(vx_l, sq_l)), isum);
   const double db = dmul(sqrt(dsq3(dsub(bx_l, bx_r), dsub(by_l, by_r), dsub(bz_l, bz_r))), isum);
   const double sl_pp = dsub(dsub(fmin(vx_l, vx_roe), cf_l), db);
   const double sr_pp = dadd(dadd(fmax(vx_r, vx_roe), cf_r), db);
+  // entropy variables (DG_solver.f90:1003-1019) formed component by component, not kept
   double da = 0.0, dbl = 0.0, dbr = 0.0;
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
+    double vls, vrs;
+    if (s == 0) {
+      vls = dfma(-ek_l, ip_l, dmul(dsub(gamma, se_l), igm1));
+      vrs = dfma(-ek_r, ip_r, dmul(dsub(gamma, se_r), igm1));
+    } else if (s < 4) {
+      vls = dmul(wl[s], ip_l);
+      vrs = dmul(wr[s], ip_r);
+    } else if (s < 7) {
+      vls = dmul(ith_l, wl[s]);
+      vrs = dmul(ith_r, wr[s]);
+    } else {
+      vls = -ith_l;
+      vrs = -ith_r;
+    }
     const double dfs = dsub(fr[s], fl[s]);
-    da = dfma(dsub(vr[s], vl[s]), dsub(wr[s], wl[s]), da);
-    dbl = dfma(vl[s], dfs, dbl);
-    dbr = dfma(vr[s], dfs, dbr);
+    da = dfma(dsub(vrs, vls), dsub(wr[s], wl[s]), da);
+    dbl = dfma(vls, dfs, dbl);
+    dbr = dfma(vrs, dfs, dbr);
   }
   const double ia = 1.0 / dadd(fmax(da, 0.0), 1e-8);
   const double def = dsub(ef_r, ef_l), jbx = dsub(bx_r, bx_l);

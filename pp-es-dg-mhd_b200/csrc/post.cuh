@@ -176,6 +176,14 @@ __device__ __forceinline__ void grp_sum8(double* a, double* row) {
   __syncwarp();  // the row is rewritten next
 }
 
+// a[v] for a lane-dependent v in 0..7, by selects (an indexed read would put a[] in local memory)
+__device__ __forceinline__ double pick8(const double* a, int v) {
+  double r = a[0];
+#pragma unroll
+  for (int q = 1; q < 8; ++q) r = (v == q) ? a[q] : r;
+  return r;
+}
+
 __device__ __forceinline__ double node_prs(const double* x, double gamma) {
   return prs_of(x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], gamma);
 }
@@ -398,11 +406,16 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
     const double* pk = bk + grp * EB + node;
     if (s1.u0) {
       const double dts = __dmul_rn(s1.coef, *s1.dt);
+      if (inner && nd) {  // the common case, one branch for all eight variables
 #pragma unroll
-      for (int v = 0; v < 8; ++v)
-        x[v] = !act ? 0.0
-                    : (inner ? __dadd_rn(pu[v * NN], __dmul_rn(dts, pk[v * NN]))
-                             : stage1_node<P>(s1, g, i, j, false, v, node, dts));
+        for (int v = 0; v < 8; ++v) x[v] = __dadd_rn(pu[v * NN], __dmul_rn(dts, pk[v * NN]));
+      } else if (act) {  // a ghost element
+#pragma unroll
+        for (int v = 0; v < 8; ++v) x[v] = stage1_node<P>(s1, g, i, j, false, v, node, dts);
+      } else {
+#pragma unroll
+        for (int v = 0; v < 8; ++v) x[v] = 0.0;
+      }
     } else {
 #pragma unroll
       for (int v = 0; v < 8; ++v) x[v] = act ? pu[v * NN] : 0.0;
@@ -460,7 +473,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
       // and the input row is read two entries at a time; the sums run over m in order
       const double2* a2 = reinterpret_cast<const double2*>(s_A) + node;
       const double2* b2 = reinterpret_cast<const double2*>(sb);
-#pragma unroll 4
+#pragma unroll
       for (int m = 0; m < N2; m += 2) {
         const double2 b = b2[m >> 1];
         const double2 a0 = a2[m * NN], a1 = a2[(m + 1) * NN];
@@ -480,8 +493,8 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
     // chunk sum of (hx*hy)*avg over interior elements in element order (DG_solver.f90:227-229)
     if (el < TE)
 #pragma unroll
-      for (int v = 0; v < 8; ++v)
-        if (v % GS == node) s_red[el * 8 + v] = inner ? (g.hx * g.hy) * avg[v] : 0.0;
+      for (int v0 = 0; v0 < 8; v0 += GS)
+        if (node + v0 < 8) s_red[el * 8 + node + v0] = inner ? (g.hx * g.hy) * pick8(avg, node + v0) : 0.0;
   }
   bool neg = false;
   if (limit) {
@@ -498,8 +511,8 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
     for (int v = 0; v < 8; ++v) u[e * EB + v * NN + node] = x[v];
   if (valid)
 #pragma unroll
-    for (int v = 0; v < 8; ++v)
-      if (v % GS == node) u_avg[e * 8 + v] = avg[v];
+    for (int v0 = 0; v0 < 8; v0 += GS)
+      if (node + v0 < 8) u_avg[e * 8 + node + v0] = pick8(avg, node + v0);
   if (NEEDG && need_global) {
     __syncthreads();
     if (tid < 8) {
