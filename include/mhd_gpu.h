@@ -186,7 +186,10 @@ int mhd_gpu_solve_begin(mhd_gpu_t *h, double final_T, double cfl, int use_oedg, 
                         int ent_offset, double *tot_ent, double *dt_lim);
 
 /* One time step of the solving loop (drive.f90:83-320) including its re-tries, entirely on the
- * device; blocks until the step is done and fills *st (may be NULL). */
+ * device; blocks until the step is done and fills *st (may be NULL).  The result is in slot 0
+ * (u_con, interior; its ghost ring is left as it was, as in the reference).  The stage slots
+ * 1..rknstg are the driver's scratch: unlike the reference's uRK_con(:,rknstg), slot rknstg does
+ * not hold a copy of the accepted interior afterwards (the final limiter writes u_con only). */
 int mhd_gpu_step(mhd_gpu_t *h, mhd_gpu_status *st);
 
 /* Up to max_steps time steps (<= 0: until final_T), queued without host round trips;

@@ -216,11 +216,13 @@ void launch_bc(mhd_gpu* h, double* u, int gate) {
   bc_kernel<P><<<grid1d(n, 256), 256, 0, h->stream>>>(u, h->geo, h->ctrl, gate);
 }
 
+// ug: the array whose ghost ring the boundary halos come from (nullptr: u's own)
 template <int P>
-void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate, StageCombine sc = StageCombine{}) {
+void launch_residual(mhd_gpu* h, const double* u, double* ut, int gate, StageCombine sc = StageCombine{},
+                     const double* ug = nullptr) {
   using L = Res2Layout<P>;
   dim3 grid((h->nx + L::TX - 1) / L::TX, (h->ny + L::TY - 1) / L::TY);
-  residual2_kernel<P><<<grid, L::NT, L::BYTES, h->stream>>>(u, ut, h->geo, h->ctrl, gate, sc);
+  residual2_kernel<P><<<grid, L::NT, L::BYTES, h->stream>>>(u, ug ? ug : u, ut, h->geo, h->ctrl, gate, sc);
 }
 
 // the re-try residual of a try (gate ST_RECOMPUTE, usually closed): a persistent grid of the CTAs
@@ -263,9 +265,11 @@ template <int P>
 // s1 (time-step pipeline, stage 1 only): loop 1 forms the stage state from u0 and the stage-1
 // residual, with its ghost ring, in place of the combination and boundary-fill launches
 // entsum_later (time-step pipeline): the entropy sum is left to the stage-end launch
+// accept_only (with accept_dst): the limiter writes its result to accept_dst only, leaving slot's
+// interior as loop 1 left it
 void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const double* dt_ptr, double oedg_dt,
                  int ent_offset, int comput_ent, double* accept_dst, int gate, int fuse = 0,
-                 Stage1Src s1 = Stage1Src{}, bool entsum_later = false) {
+                 Stage1Src s1 = Stage1Src{}, bool entsum_later = false, int accept_only = 0) {
   const int nb1 = pp_nblk_avg<P>(h);
   const int limit_in_loop1 = fuse && !apply_oedg && !comput_ent && !accept_dst;
   if (apply_oedg) {
@@ -293,7 +297,7 @@ void launch_post(mhd_gpu* h, int slot, int apply_oedg, int apply_ldf, const doub
   pp_limit_kernel<P><<<g3, PPCfg<P>::NT, 0, h->stream>>>(h->u[slot], h->u_avg, h->geo, h->ctrl, gate, apply_oedg, dt_ptr,
                                                    oedg_dt, ent_offset, comput_ent, h->sig_x, h->sig_y,
                                                    h->cell_ent_DG, h->cell_ent_FV, h->cell_ent_nan,
-                                                   h->ent_partial, accept_dst);
+                                                   h->ent_partial, accept_dst, accept_only);
   if (comput_ent && !entsum_later)
     pp_entsum_kernel<<<1, 256, 0, h->stream>>>(h->ent_partial, (int)(g3.x * g3.y), h->ctrl, gate);
 }
@@ -396,13 +400,20 @@ void enqueue_try(mhd_gpu* h) {
     if (s > 1 && R > 3) launch_combine<P>(h, s, &h->ctrl->dt, 0.0, ST_RUN);
     if (s > 1) launch_bc<P>(h, h->u[s], ST_RUN);
     const Stage1Src s1 = s == 1 ? Stage1Src{h->u[0], h->ut[1], &h->ctrl->dt, stage1_coef(R)} : Stage1Src{};
+    // the final stage's limiter writes the accepted interior to u_con only (drive.f90:304-311); the
+    // stage array's ghost ring is then filled from u_con, and the next step's stage-1 residual reads
+    // u_con's interior with that ring.  u_con keeps its own ghost ring, which only the re-try
+    // residual reads (drive.f90:104 takes u_con as it is).
     launch_post<P>(h, s, h->use_oedg && fin, h->use_ldf, &h->ctrl->dt, 0.0, h->ent_offset, fin,
-                   fin ? h->u[0] : nullptr, ST_RUN, 1, s1, /*entsum_later=*/true);
+                   fin ? h->u[0] : nullptr, ST_RUN, 1, s1, /*entsum_later=*/true, /*accept_only=*/fin);
+    const double* cur = fin ? h->u[0] : h->u[s];  // the stage result's interior
     // entropy sum (final stage), stage-end decision, next stage's pseudo-time and the ghost ring
     stage_end_bc_kernel<P><<<grid1d(nghost, 256), 256, 0, h->stream>>>(
-        h->u[s], h->geo, h->ctrl, R, s, fin ? 0 : s + 1, fin ? h->ent_partial : nullptr, nseg, h->log, h->log_cap);
-    if (h->diag) launch_diag<P>(h, h->u[s], ST_RUN);
-    launch_residual<P>(h, h->u[s], h->ut[(s % R) + 1], ST_RUN, fin ? StageCombine{} : next_stage_combine(h, s + 1));
+        cur, h->u[s], h->geo, h->ctrl, R, s, fin ? 0 : s + 1, fin ? h->ent_partial : nullptr, nseg, h->log,
+        h->log_cap);
+    if (h->diag) launch_diag<P>(h, cur, ST_RUN);
+    launch_residual<P>(h, cur, h->ut[(s % R) + 1], ST_RUN, fin ? StageCombine{} : next_stage_combine(h, s + 1),
+                       h->u[s]);
   }
   ctl_step_end<<<1, 1, 0, h->stream>>>(h->ctrl, R, h->log, h->log_cap);
 }
@@ -1109,17 +1120,17 @@ extern "C" int mhd_gpu_semidiscretize_noalloc(int p, int nx, int ny, double hx, 
   switch (p) {
     case 1: {
       using L = Res2Layout<1>;
-      residual2_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
+      residual2_kernel<1><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     case 2: {
       using L = Res2Layout<2>;
-      residual2_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
+      residual2_kernel<2><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
     default: {
       using L = Res2Layout<3>;
-      residual2_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
+      residual2_kernel<3><<<dim3((nx + L::TX - 1) / L::TX, (ny + L::TY - 1) / L::TY), L::NT, L::BYTES, s>>>(u, u, ut, g, ctrl, GATE_ALWAYS, StageCombine{});
       break;
     }
   }

@@ -56,9 +56,10 @@ __device__ __forceinline__ BcSrc bc_source(const Geo& g, int i, int j, int v, in
   return s;
 }
 
-// Ghost-ring fill.  One thread per ghost value; corners untouched.
+// Ghost-ring fill of dst from the interior of src (the same array, or an array whose interior holds
+// the same values).  One thread per ghost value; corners untouched.
 template <int P>
-__device__ __forceinline__ void bc_value(double* __restrict__ u, const Geo& g, long long it) {
+__device__ __forceinline__ void bc_value(const double* src, double* dst_u, const Geo& g, long long it) {
   constexpr int N = P + 1, NN = N * N, EB = 8 * NN;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long nghost = 2LL * (nx + ny);
@@ -73,17 +74,17 @@ __device__ __forceinline__ void bc_value(double* __restrict__ u, const Geo& g, l
   const long long dst = ((long long)j * NXG + i) * EB + vi;
   const BcSrc s = bc_source<P>(g, i, j, v, q);
   if (s.fixed) {
-    u[dst] = g.bc_state[v];
+    dst_u[dst] = g.bc_state[v];
     return;
   }
-  const double x = u[((long long)s.sj * NXG + s.si) * EB + v * NN + s.sq];
-  u[dst] = s.neg ? -x : x;
+  const double x = src[((long long)s.sj * NXG + s.si) * EB + v * NN + s.sq];
+  dst_u[dst] = s.neg ? -x : x;
 }
 
 template <int P>
 __global__ void __launch_bounds__(256) bc_kernel(double* __restrict__ u, Geo g, const Ctrl* ctrl, int gate) {
   if (!gate_open(ctrl, gate)) return;
-  bc_value<P>(u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  bc_value<P>(u, u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // many instances: items = every member's blocks of 256 ghost values
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(256) bc_batched(const InstDesc* __restrict__ i
     const int m = it.m, chunk = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
-    bc_value<P>(d.u[slot], d.g, (long long)chunk * 256 + threadIdx.x);
+    bc_value<P>(d.u[slot], d.u[slot], d.g, (long long)chunk * 256 + threadIdx.x);
   }
 }
 

@@ -200,7 +200,8 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
                                               long long ce, const Geo& g, Ctrl* ctrl, int ent_offset,
                                               int comput_ent, const double* __restrict__ cell_ent_DG,
                                               const double* __restrict__ cell_ent_FV,
-                                              const unsigned char* __restrict__ cell_ent_nan, bool* negcell) {
+                                              const unsigned char* __restrict__ cell_ent_nan, bool* negcell,
+                                              bool* scaled = nullptr) {
   using C = PPCfg<P>;
   constexpr int N = C::N, GS = C::GS;
   constexpr double BIG = 1.7976931348623157e308;
@@ -224,6 +225,7 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
     thp = fmax(fmin((pa - PP_EPS) / (pa - pmin), 1.0), 0.0);
   }
   *negcell = lead && active && (thd >= 0.0 || thp >= 0.0);  // neg_node (DG_solver.f90:602)
+  if (scaled) *scaled = active && (thd >= 0.0 || thp >= 0.0);  // this lane's node values changed
   if (active && thp >= 0.0)
 #pragma unroll
     for (int v = 0; v < 8; ++v) x[v] = avg[v] + thp * (x[v] - avg[v]);
@@ -258,6 +260,7 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
         const double th = fmax(fmin((old - eavg) / (nw - eavg), 1.0), 0.0);
 #pragma unroll
         for (int v = 0; v < 8; ++v) x[v] = avg[v] + th * (x[v] - avg[v]);
+        if (scaled) *scaled = true;
       }
     }
   }
@@ -496,19 +499,27 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
       for (int v0 = 0; v0 < 8; v0 += GS)
         if (node + v0 < 8) s_red[el * 8 + node + v0] = inner ? (g.hx * g.hy) * pick8(avg, node + v0) : 0.0;
   }
-  bool neg = false;
+  bool neg = false, scaled = false;
   if (limit) {
     __syncwarp();  // the group's lane 0 wrote the cell entropies limit_group reads
     limit_group<P>(x, avg, inner && nd, inner && node == 0, node, e, g, ctrl, ent_offset, 0, cell_ent_DG, cell_ent_FV,
-                   cell_ent_nan, &neg);
+                   cell_ent_nan, &neg, &scaled);
     const unsigned cnt = __popc(__ballot_sync(FULL_MASK, neg));
     if (lane == 0 && cnt) atomicAdd(s_cnt, (int)cnt);
   }
-  // write back state and averages of the admissible elements (the state of every element when
-  // it was formed here)
-  if ((valid || s1.u0) && act)
+  // write back the state of every element formed here, and of an admissible element what changed
+  // in place: (Bx, By) after the LDF, all eight variables where the limiter scaled the element
+  // (the positivity and entropy-offset scalings are conditional, so most elements keep six of
+  // their eight variables bit for bit and need not store them)
+  if (act) {
+    if (s1.u0 || scaled) {
 #pragma unroll
-    for (int v = 0; v < 8; ++v) u[e * EB + v * NN + node] = x[v];
+      for (int v = 0; v < 8; ++v) u[e * EB + v * NN + node] = x[v];
+    } else if (valid && apply_ldf) {
+      u[e * EB + 4 * NN + node] = x[4];
+      u[e * EB + 5 * NN + node] = x[5];
+    }
+  }
   if (valid)
 #pragma unroll
     for (int v0 = 0; v0 < 8; v0 += GS)
@@ -909,7 +920,7 @@ __device__ __forceinline__ void pp_limit_segment(
     int apply_oedg, double oedg_dt, int ent_offset, int comput_ent, const double* __restrict__ sig_x,
     const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
     const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
-    double* __restrict__ ent_out, double* __restrict__ accept_dst, double* s_ent, int* s_cnt) {
+    double* __restrict__ ent_out, double* __restrict__ accept_dst, int accept_only, double* s_ent, int* s_cnt) {
   using C = PPCfg<P>;
   constexpr int NN = C::NN, EB = C::EB, GS = C::GS, G = C::G, TE = C::TE;
   if (ctrl->neg_avg) return;  // the reference skips loop 3 once neg_avg is set (DG_solver.f90:431)
@@ -975,7 +986,7 @@ __device__ __forceinline__ void pp_limit_segment(
   if (act)
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
-      u[e * EB + v * NN + node] = x[v];
+      if (!accept_only) u[e * EB + v * NN + node] = x[v];
       if (accept_dst) accept_dst[e * EB + v * NN + node] = x[v];
     }
   if (comput_ent) {  // chunk partial in element order
@@ -996,7 +1007,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
                     int ent_offset, int comput_ent, const double* __restrict__ sig_x,
                     const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
                     const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
-                    double* __restrict__ ent_partial, double* __restrict__ accept_dst) {
+                    double* __restrict__ ent_partial, double* __restrict__ accept_dst, int accept_only) {
   __shared__ double s_ent[PPCfg<P>::TE];
   __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
@@ -1005,7 +1016,8 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
   const double oedg_dt = dt_ptr ? *dt_ptr : oedg_dt_arg;
   pp_limit_segment<P>(u, u_avg, g, ctrl, blockIdx.x, blockIdx.y, apply_oedg, oedg_dt, ent_offset, comput_ent,
                       sig_x, sig_y, cell_ent_DG, cell_ent_FV, cell_ent_nan,
-                      ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst, s_ent, &s_cnt);
+                      ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst, accept_only, s_ent,
+                      &s_cnt);
   __syncthreads();
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
 }
@@ -1029,7 +1041,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     const int seg = local % nseg, row = local / nseg;
     pp_limit_segment<P>(d.u[slot], d.u_avg, d.g, d.ctrl, seg, row, d.use_oedg && final, d.ctrl->dt,
                         d.ent_offset, final, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
-                        d.ent_partial + local, final ? d.u[0] : nullptr, s_ent, &s_cnt);
+                        d.ent_partial + local, final ? d.u[0] : nullptr, 0, s_ent, &s_cnt);
     __syncthreads();
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
@@ -1058,8 +1070,10 @@ __device__ __forceinline__ void pp_entsum_body(const double* __restrict__ partia
 // skips its fill, and a fill of an abandoned stage only writes scratch ghosts, so the result is
 // that of the separate launches in sequence.
 // The stage's record goes to the driver log (log may be nullptr).
+// src: the array whose interior the ghost ring is filled from (u itself, or u_con after the final
+// stage, whose limiter writes the accepted interior to u_con only).
 template <int P>
-__global__ void __launch_bounds__(256) stage_end_bc_kernel(double* __restrict__ u, Geo g, Ctrl* ctrl, int R,
+__global__ void __launch_bounds__(256) stage_end_bc_kernel(const double* src, double* u, Geo g, Ctrl* ctrl, int R,
                                                           int stage, int next_stage,
                                                           const double* __restrict__ ent_partial, int ent_nblk,
                                                           LogEntry* log, int log_cap) {
@@ -1081,7 +1095,7 @@ __global__ void __launch_bounds__(256) stage_end_bc_kernel(double* __restrict__ 
   } else {
     run = *reinterpret_cast<volatile const int*>(&ctrl->state) == ST_RUN;
   }
-  if (run) bc_value<P>(u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  if (run) bc_value<P>(src, u, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void __launch_bounds__(256) pp_entsum_kernel(const double* __restrict__ partial, int nblk,
@@ -1106,7 +1120,7 @@ __global__ void __launch_bounds__(256) stage_end_bc_batched(const InstDesc* __re
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
     const InstDesc& d = insts[it.m];
     if (*reinterpret_cast<volatile const int*>(&d.ctrl->state) != ST_RUN) continue;
-    bc_value<P>(d.u[slot], d.g, (long long)it.local() * 256 + threadIdx.x);
+    bc_value<P>(d.u[slot], d.u[slot], d.g, (long long)it.local() * 256 + threadIdx.x);
   }
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const InstDesc& d = insts[i];

@@ -134,11 +134,14 @@ __device__ __forceinline__ double group_max(double v, int gbase) {
 
 // One tile (elements tile_x*TX + 1 .., tile_y*TY + 1 ..).  `phase` = the parity of the tile
 // barrier's next phase (flipped here).  Returns false if the wait for the tile's copies ran out
-// (FLAG_DEVICE_WAIT is then set): the caller must stop.
+// (FLAG_DEVICE_WAIT is then set): the caller must stop.  ug = the array whose ghost ring the
+// boundary halos come from (u itself, or the last stage array whose ring was filled from u's
+// interior after the final stage; the interior always comes from u).
 template <int P>
-__device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, double* __restrict__ ut,
-                                               const Geo& g, Ctrl* ctrl, int tile_x, int tile_y, double* sm,
-                                               unsigned& phase, const StageCombine& sc = StageCombine{}) {
+__device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, const double* __restrict__ ug,
+                                               double* __restrict__ ut, const Geo& g, Ctrl* ctrl, int tile_x,
+                                               int tile_y, double* sm, unsigned& phase,
+                                               const StageCombine& sc = StageCombine{}) {
   using L = Res2Layout<P>;
   constexpr int N = L::N, NN = L::NN, EB = L::EB, ES = L::ES, TX = L::TX, TY = L::TY, TE = L::TE;
   constexpr int NT = L::NT, NW = L::NW, G = L::G;
@@ -188,19 +191,24 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
       }
     }
   }
+  // a halo side on the domain boundary reads the ghost ring (of ug)
+  const double* uxl = i0 == 1 ? ug : u;
+  const double* uxr = i0 + W == nx + 1 ? ug : u;
+  const double* uyb = j0 == 1 ? ug : u;
+  const double* uyt = j0 + H == ny + 1 ? ug : u;
   for (int it = tid; it < TY * 8 * N; it += NT) {  // x halos: traces k = n-1 (left) / 0 (right)
     const int r = it / (8 * N), rem = it - r * 8 * N, v = rem / N, l = rem - v * N;
     if (r < H) {
-      const double* rowp = u + (long long)(j0 + r) * rowstride;
-      s_hxl[it] = __ldg(rowp + (long long)(i0 - 1) * EB + v * NN + (N - 1) + N * l);
-      s_hxr[it] = __ldg(rowp + (long long)(i0 + W) * EB + v * NN + 0 + N * l);
+      const long long row = (long long)(j0 + r) * rowstride;
+      s_hxl[it] = __ldg(uxl + row + (long long)(i0 - 1) * EB + v * NN + (N - 1) + N * l);
+      s_hxr[it] = __ldg(uxr + row + (long long)(i0 + W) * EB + v * NN + 0 + N * l);
     }
   }
   for (int it = tid; it < TX * 8 * N; it += NT) {  // y halos: traces l = n-1 (bottom) / 0 (top)
     const int c = it / (8 * N), rem = it - c * 8 * N, v = rem / N, k = rem - v * N;
     if (c < W) {
-      s_hyb[it] = __ldg(u + (long long)(j0 - 1) * rowstride + (long long)(i0 + c) * EB + v * NN + k + N * (N - 1));
-      s_hyt[it] = __ldg(u + (long long)(j0 + H) * rowstride + (long long)(i0 + c) * EB + v * NN + k);
+      s_hyb[it] = __ldg(uyb + (long long)(j0 - 1) * rowstride + (long long)(i0 + c) * EB + v * NN + k + N * (N - 1));
+      s_hyt[it] = __ldg(uyt + (long long)(j0 + H) * rowstride + (long long)(i0 + c) * EB + v * NN + k);
     }
   }
   {
@@ -488,16 +496,16 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, dou
   return true;
 }
 
-// single instance: one CTA per tile
+// single instance: one CTA per tile (ug: the ghost-ring source, see residual_tile2)
 template <int P>
 __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
-    residual2_kernel(const double* __restrict__ u, double* __restrict__ ut, Geo g, Ctrl* ctrl, int gate,
-                     StageCombine sc) {
+    residual2_kernel(const double* __restrict__ u, const double* __restrict__ ug, double* __restrict__ ut, Geo g,
+                     Ctrl* ctrl, int gate, StageCombine sc) {
   if (!gate_open(ctrl, gate)) return;
   extern __shared__ __align__(16) double sm[];
   res2_prologue<P>(sm);
   unsigned phase = 0;
-  residual_tile2<P>(u, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, phase, sc);
+  residual_tile2<P>(u, ug, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, phase, sc);
 }
 
 // single instance, persistent: CTA b computes tiles b, b + gridDim.x, ... (row-major, ntx per row).
@@ -512,7 +520,7 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
   res2_prologue<P>(sm);
   unsigned phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    if (!residual_tile2<P>(u, ut, g, ctrl, t % ntx, t / ntx, sm, phase, StageCombine{})) return;
+    if (!residual_tile2<P>(u, u, ut, g, ctrl, t % ntx, t / ntx, sm, phase, StageCombine{})) return;
     __syncthreads();  // the next tile reuses shared memory
   }
 }
@@ -537,7 +545,8 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
     if (!gate_open(d.ctrl, gate)) continue;
     const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
     const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
-    if (!residual_tile2<P>(d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc)) return;
+    if (!residual_tile2<P>(d.u[src], d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc))
+      return;
     __syncthreads();  // the next tile reuses shared memory
   }
 }

@@ -175,7 +175,9 @@ def test_blast400_to_final_time(pkg, ora):
         st = g.advance(chunk, check_every=16)
         for s in (1, 2, 3):
             us = g.download_state(s)
-            ref = np.asfortranarray(us.copy())
+            # the final stage's limiter writes the accepted interior to u_con only, and the last
+            # stage array's ring is filled from there
+            ref = np.asfortranarray((g.download_state(0) if s == 3 else us).copy())
             o.apply_bc(ref)
             ghost = np.isfinite(ref)
             ghost[:, :, :, 1:-1, 1:-1] = False
