@@ -35,10 +35,10 @@ import build as B  # noqa: E402
 # group -> macro(s) -> per degree the candidates; set i takes candidate i of every degree
 GROUPS = {
     "residual": {
-        "MHD_RES2_CFG": {
-            1: [(8, 8, 256, 2), (8, 4, 128, 4), (8, 6, 192, 3), (16, 4, 256, 2)],
-            2: [(6, 4, 256, 2), (4, 3, 128, 4), (6, 3, 192, 3), (8, 3, 256, 2)],
-            3: [(4, 4, 256, 2), (4, 2, 128, 4), (4, 3, 192, 3), (8, 2, 256, 2)],
+        "MHD_RES2_CFG": {  # 128 threads at 4, 5 and 6 CTAs per SM (128, 102, 85 registers), 256 at 3
+            1: [(8, 4, 128, 4), (8, 4, 128, 5), (8, 4, 128, 6), (8, 8, 256, 3)],
+            2: [(4, 3, 128, 4), (4, 3, 128, 5), (4, 3, 128, 6), (6, 4, 256, 3)],
+            3: [(4, 2, 128, 4), (4, 2, 128, 5), (4, 2, 128, 6), (8, 2, 256, 3)],
         },
     },
     "post": {
@@ -151,11 +151,29 @@ def tune(group, jobs):
             print(f"{group} set {i}: {times[i]}", flush=True)
     if not times:
         sys.exit(f"no {group} candidate set could be timed")
+    write_header(group, times)
+
+
+MARGIN = 0.01  # run-to-run spread of these timings on one GPU
+
+
+def pick(times, p):
+    """the fastest set for degree p; set 0 (the incumbent) unless another beats it by more than
+    MARGIN, so that timing noise does not swap in a candidate with more spilled registers"""
+    best = min(times, key=lambda i: times[i][p])
+    if 0 in times and times[best][p] >= (1.0 - MARGIN) * times[0][p]:
+        return 0
+    return best
+
+
+def write_header(group, times):
+    """times[set][p] in ms -> the group's header with the chosen candidate per degree"""
     unit = "residual ms per launch" if group == "residual" else "ms per SSP-RK3 step (OEDG + LDF + PP)"
     lines = [f"// {HEADERS[group]} -- written by autotune.py: the fastest candidate per degree on this GPU",
-             f"// ({unit}, vortex mesh of about 33 M DOFs)."]
+             f"// ({unit}, vortex mesh of about 33 M DOFs; set 0 stays unless another is faster by more",
+             f"// than {100 * MARGIN:.0f} %)."]
     for p in (1, 2, 3):
-        best = min(times, key=lambda i: times[i][p])
+        best = pick(times, p)
         for i in sorted(times):
             knobs = "; ".join(f"{m} {GROUPS[group][m][p][i]}" for m in GROUPS[group])
             lines.append(f"//   p={p} {knobs}: {times[i][p]:.4f} ms{'  <- chosen' if i == best else ''}")
