@@ -17,9 +17,12 @@ horizon), giving each request
   * T_ideal = steps x 3 x DOFs / R_peak, the time at the best throughput measured on the grid.
 
 sum(T_solo) / sum(T_ideal) bounds the solves/s gain of any batched or served form over one run at a
-time on this mix (Amdahl: a batch cannot make a run faster than the device's peak rate).
+time on this mix (Amdahl: a batch cannot make a run faster than the device's peak rate).  R_peak is
+the best rate of the grid, or --device-peak (the rate a mesh that fills the GPU reaches, e.g. the
+512x512 p=3 vortex), which bounds a batch of small meshes that together fill the GPU.
 
-    python tests/study_serving_bound.py [--n-lo 32] [--n-hi 512] [--samples 20000] [--json out]
+    python tests/study_serving_bound.py [--n-lo 32] [--n-hi 512] [--samples 20000] [--device-peak R]
+                                        [--json out]
 """
 import argparse
 import json
@@ -65,6 +68,7 @@ def main():
     ap.add_argument("--n-hi", type=int, default=512)
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--device-peak", type=float, default=0.0, help="DOF-stage/s (0: the grid's best)")
     ap.add_argument("--json", default=None)
     a = ap.parse_args()
     import __graft_entry__
@@ -79,6 +83,7 @@ def main():
                     print(json.dumps(dict(problem=name, p=p, n=n, ms_per_step=ms, dt=dt,
                                           dof_stage_per_s=3 * 8 * n * n * (p + 1) ** 2 / (ms * 1e-3))), flush=True)
     peak = max(3 * 8 * n * n * (p + 1) ** 2 / (ms * 1e-3) for (name, p, n), (ms, dt) in grid.items())
+    peak = max(peak, a.device_peak)
 
     def interp(name, p, n, k):  # k = 0: ms per step, 1: dt x n (dt scales as 1/n)
         ns = sorted(m for (nm, pp, m) in grid if nm == name and pp == p)
