@@ -298,7 +298,13 @@ def serve(pkg, reqs, batched, budget, tries_per_round=2):
     tts = np.array([x["finished"] - x["arrival"] for x in res])
     makespan = max(x["finished"] for x in res) - min(x["arrival"] for x in res)
     ok = sum(1 for x in res if x["done"] == 1 and x["flags"] == 0 and x["error"] == 0)
-    return {"solves_per_s": len(res) / makespan, "p50_tts_s": float(np.percentile(tts, 50)),
+    # steady state: completions between the 10 % and the 90 % mark over that window (the ramp-up
+    # and the tail, where the last runs execute nearly alone, left out)
+    fin = np.sort(np.array([x["finished"] for x in res]))
+    i10, i90 = int(0.1 * len(fin)), int(0.9 * len(fin)) - 1
+    steady = (i90 - i10) / (fin[i90] - fin[i10]) if i90 > i10 and fin[i90] > fin[i10] else None
+    return {"solves_per_s": len(res) / makespan, "steady_solves_per_s": steady,
+            "p50_tts_s": float(np.percentile(tts, 50)),
             "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok, "requests": len(reqs),
             "wall_s": wall, "steps": int(sum(x["steps"] for x in res)),
             "host_s": {k: round(stats[k], 4) for k in ("admit_s", "launch_s", "wait_s", "retire_s", "idle_s")},
@@ -315,26 +321,38 @@ def pinned_copy(a):
     return out
 
 
-def serve_leg(pkg, n_req, rate, n_hi, t_scale, seed=7, n_lo=32, budget=64 << 30):
-    """one request stream served twice, batched and one run at a time, after an untimed pass of each
-    (first-touch costs: module loading, the arena reservation).  Initial states sit in pinned host
-    memory, as a serving host would keep its request buffers."""
-    reqs = make_requests(n_req, rate, seed, n_lo, n_hi, t_scale)
-    for r in reqs:
+def serve_leg(pkg, n_req, rates, n_hi, t_scale, seed=7, n_lo=32, budget=64 << 30):
+    """one request stream served at each arrival rate in `rates`, batched and one run at a time,
+    after an untimed pass of each (first-touch costs: module loading, the arena reservation).  The
+    requests (problem, mesh, degree, t_end) are the same at every rate; only the Poisson arrival
+    times scale with 1/rate.  Initial states sit in pinned host memory, as a serving host would
+    keep its request buffers."""
+    base = make_requests(n_req, 1.0, seed, n_lo, n_hi, t_scale)
+    for r in base:
         r["u0"] = pinned_copy(pkg.problems.make(r["name"]).initial_state(r["n"], r["n"], r["p"]))
-    serve(pkg, reqs[: max(4, n_req // 8)], True, budget)
-    serve(pkg, reqs[: max(4, n_req // 8)], False, budget)
-    b = serve(pkg, reqs, True, budget)
-    q = serve(pkg, reqs, False, budget)
-    return {"batched": b, "one_at_a_time": q, "speedup_solves_per_s": b["solves_per_s"] / q["solves_per_s"],
-            "stream": f"{n_req} requests, Poisson {rate:g}/s, seed {seed}, N log-uniform [{n_lo},{n_hi}], "
-                      f"p in 1..3, problem in {{OT, rotor, blast}}, t_end U[0.05,0.5] x horizon x {t_scale:g}"}
+    # the untimed pass: the first requests at the fastest rate (base arrivals are at 1/s)
+    warm = [dict(r, arrival=r["arrival"] / max(rates)) for r in base[: max(4, min(64, n_req // 8))]]
+    serve(pkg, warm, True, budget)
+    serve(pkg, warm, False, budget)
+    out = {"stream": f"{n_req} requests, Poisson arrivals, seed {seed}, N log-uniform [{n_lo},{n_hi}], "
+                     f"p in 1..3, problem in {{OT, rotor, blast}}, t_end U[0.05,0.5] x horizon x {t_scale:g}"}
+    for rate in rates:
+        reqs = [dict(r, arrival=r["arrival"] / rate) for r in base]
+        b = serve(pkg, reqs, True, budget)
+        q = serve(pkg, reqs, False, budget)
+        bs, qs = b["steady_solves_per_s"], q["steady_solves_per_s"]
+        out[f"rate_{rate:g}"] = {"batched": b, "one_at_a_time": q,
+                                 "speedup_solves_per_s": b["solves_per_s"] / q["solves_per_s"],
+                                 "speedup_steady": bs / qs if bs and qs else None}
+    return out
 
 
 # the served configuration of the scope table (N up to 512; t_end scaled by 0.05 so that the largest
-# runs finish in seconds), and a stream of small meshes, where packing runs into one launch pays most
-SERVE_STREAMS = {"spec_N32-512": dict(n_req=64, rate=200.0, n_hi=512, t_scale=0.05),
-                 "small_N32-96": dict(n_req=128, rate=2000.0, n_hi=96, t_scale=0.5)}
+# runs finish in seconds), and a stream of 1,000 small meshes with the scope table's t_end at two
+# arrival rates (one that a single run at a time cannot keep up with, one that saturates both
+# modes), where packing runs into one launch pays most
+SERVE_STREAMS = {"spec_N32-512": dict(n_req=64, rates=[200.0], n_hi=512, t_scale=0.05),
+                 "small_N32-96": dict(n_req=1000, rates=[100.0, 2000.0], n_hi=96, t_scale=1.0)}
 
 
 def batched_leg(pkg, n_runs=512, steps=4, seed=11, n_lo=32, n_hi=256, sample=8):
@@ -535,12 +553,25 @@ def run_ours(args):
         }
         if e2e:
             line["e2e"] = e2e
+        t_leg = time.perf_counter()
+
+        def progress(leg):  # wall time of each extra leg, on stderr (stdout carries the JSON line)
+            nonlocal t_leg
+            now = time.perf_counter()
+            print(f"bench: {leg} leg {now - t_leg:.1f} s", file=sys.stderr, flush=True)
+            t_leg = now
+
         if not args.no_batched and ws == 1:
             line["batched"] = batched_leg(pkg)
+            progress("batched")
         if not args.no_serve and ws == 1:
-            line["served"] = {k: serve_leg(pkg, **kw) for k, kw in SERVE_STREAMS.items()}
+            line["served"] = {}
+            for k, kw in SERVE_STREAMS.items():
+                line["served"][k] = serve_leg(pkg, **kw)
+                progress(f"served {k}")
         if not args.no_cpu and ws == 1:
             line["cpu_baseline"] = cpu_sample(prob_name, n, p, oedg, ldf, budget_s=args.cpu_budget)
+            progress("cpu baseline")
         print(json.dumps(line), flush=True)
     solver.close()
     if dist:
