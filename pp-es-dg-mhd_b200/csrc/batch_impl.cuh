@@ -103,7 +103,8 @@ void member_work(const mhd_gpu* h, long long* cnt, InstDesc& d) {
   d.nblk_avg = (int)((nelg + TE - 1) / TE);
   cnt[WK_AVG] = d.nblk_avg;
   cnt[WK_SIG] = ((nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX) * ((ny + SigCfg<P>::TY - 1) / SigCfg<P>::TY);
-  d.nseg_limit = (int)(((nx + TE - 1) / TE) * ny);
+  constexpr int TEL = PPCfg<P>::TEL;  // the limiter's row segments
+  d.nseg_limit = (int)(((nx + TEL - 1) / TEL) * ny);
   cnt[WK_LIM] = d.nseg_limit;
   cnt[WK_CMB] = (nx * ny * EB + 255) / 256;
   cnt[WK_BC] = (2 * (nx + ny) * EB + 255) / 256;

@@ -126,7 +126,7 @@ int grid1d(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 template <int P>
 int pp_nblk_avg(const mhd_gpu* h) { return grid1d((long long)(h->nx + 2) * (h->ny + 2), PPCfg<P>::TE); }
 template <int P>
-dim3 pp_grid_limit(const mhd_gpu* h) { return dim3((h->nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE, h->ny); }
+dim3 pp_grid_limit(const mhd_gpu* h) { return dim3((h->nx + PPCfg<P>::TEL - 1) / PPCfg<P>::TEL, h->ny); }
 
 // CTAs of pp_avg_ldf_kernel<P> the device holds at once (its grid walks the chunks)
 template <int P, bool NEEDG>

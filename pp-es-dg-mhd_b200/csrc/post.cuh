@@ -87,15 +87,38 @@ struct PPTune<3> {
   static constexpr SigParams sig{MHD_SIG_CFG3};
 };
 
+// Lanes per element: loop 1 takes a power-of-two group of GS lanes (16 for the 9 nodes of p = 2);
+// the final stage's limiter kernel takes GSL lanes, 9 at p = 2 (three elements per warp, lanes
+// 27-31 idle), where its per-node work outweighs the dearer reductions of a 9-lane group (measured
+// on the 400x400 p = 2 blast: limiter 0.115 -> 0.088 ms; loop 1 with 9-lane groups and its cell
+// sums through shared memory was 3 % slower and stays at 16 lanes).
 template <int P>
 struct PPCfg {
   static constexpr int N = P + 1, NN = N * N, EB = 8 * NN, N2 = 2 * NN;
   static constexpr int NT = PPTune<P>::pp.NT, MINB = PPTune<P>::pp.MINB;
-  static constexpr int GS = NN <= 4 ? 4 : (NN <= 8 ? 8 : (NN <= 16 ? 16 : 32));  // lanes per element
+  static constexpr int GS = NN <= 4 ? 4 : (NN <= 8 ? 8 : (NN <= 16 ? 16 : 32));  // loop 1: lanes per element
   static constexpr int G = 32 / GS;                                               // elements per warp
   static constexpr int TE = (NT / 32) * G;                                        // elements per CTA chunk
+  static constexpr int GSL = NN == 9 ? 9 : GS;                                    // limiter kernel: lanes per element
+  static constexpr int GL = 32 / GSL;
+  static constexpr int TEL = (NT / 32) * GL;                                      // elements per limiter CTA
   static_assert(NT % 32 == 0 && NT <= 1024, "whole warps");
 };
+
+// This lane's group and node for groups of GS lanes.  Where GS does not divide 32 the lanes past
+// the last group are idle: they take group 0's lanes as partners in the group reductions (their
+// results are unused) and a node number beyond every element (node >= NN).
+template <int GS>
+struct GrpLane {
+  int grp, node;
+  bool idle;
+};
+template <int GS>
+__device__ __forceinline__ GrpLane<GS> grp_lane() {
+  const int lane = threadIdx.x & 31, g = lane / GS;
+  const bool idle = g >= 32 / GS;
+  return GrpLane<GS>{idle ? 0 : g, idle ? lane : lane - g * GS, idle};
+}
 // the smallest chunk of any degree: per-chunk partial buffers are sized by it
 constexpr int pp_min_chunk() {
   return PPCfg<1>::TE < PPCfg<2>::TE ? (PPCfg<1>::TE < PPCfg<3>::TE ? PPCfg<1>::TE : PPCfg<3>::TE)
@@ -115,24 +138,44 @@ __device__ __forceinline__ void cp_async16(double* dst_shared, const double* src
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int GS>
-__device__ __forceinline__ double grp_sum(double v) {
+// Reduction over a group of GS lanes, the result in every lane of the group.  A power-of-two group
+// uses the xor butterfly.  Otherwise (GS = 9) the lanes past the largest power of two P2 are
+// folded onto the group's first lanes, the P2 lanes reduce by a butterfly with partners inside the
+// group (explicit lane indices), and every lane takes the group's first lane's result: a fixed
+// order, and one value for the whole group.
+template <int GS, class Op>
+__device__ __forceinline__ double grp_reduce(double v, Op op) {
+  if constexpr ((GS & (GS - 1)) == 0) {
 #pragma unroll
-  for (int o = GS / 2; o > 0; o >>= 1) v = v + __shfl_xor_sync(FULL_MASK, v, o);
-  return v;
-}
-template <int GS>
-__device__ __forceinline__ double grp_min(double v) {
+    for (int o = GS / 2; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(FULL_MASK, v, o));
+    return v;
+  } else {
+    constexpr int P2 = GS >= 16 ? 16 : (GS >= 8 ? 8 : (GS >= 4 ? 4 : 2));
+    static_assert(GS - P2 <= P2, "one fold");
+    const GrpLane<GS> gl = grp_lane<GS>();
+    const int gb = gl.grp * GS, node = gl.node;
+    const double hi = __shfl_sync(FULL_MASK, v, gb + (node + P2 < GS ? node + P2 : 0));
+    if (node + P2 < GS) v = op(v, hi);
 #pragma unroll
-  for (int o = GS / 2; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL_MASK, v, o));
-  return v;
+    for (int o = P2 / 2; o > 0; o >>= 1) v = op(v, __shfl_sync(FULL_MASK, v, gb + ((node ^ o) & (P2 - 1))));
+    return __shfl_sync(FULL_MASK, v, gb);
+  }
 }
+struct OpAdd {
+  __device__ __forceinline__ double operator()(double a, double b) const { return a + b; }
+};
+struct OpMin {
+  __device__ __forceinline__ double operator()(double a, double b) const { return fmin(a, b); }
+};
+struct OpMax {
+  __device__ __forceinline__ double operator()(double a, double b) const { return fmax(a, b); }
+};
 template <int GS>
-__device__ __forceinline__ double grp_max(double v) {
-#pragma unroll
-  for (int o = GS / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
-  return v;
-}
+__device__ __forceinline__ double grp_sum(double v) { return grp_reduce<GS>(v, OpAdd{}); }
+template <int GS>
+__device__ __forceinline__ double grp_min(double v) { return grp_reduce<GS>(v, OpMin{}); }
+template <int GS>
+__device__ __forceinline__ double grp_max(double v) { return grp_reduce<GS>(v, OpMax{}); }
 
 // All eight sums of a[0..7] over each group of GS lanes, in every lane of the group, by a
 // reduce-scatter (each exchange halves the values a lane carries, one lane bit per level: 8
@@ -142,6 +185,7 @@ __device__ __forceinline__ double grp_max(double v) {
 // and read from the one copy in `row`).
 template <int GS>
 __device__ __forceinline__ void grp_sum8(double* a, double* row) {
+  static_assert((GS & (GS - 1)) == 0, "power-of-two groups");
   constexpr int LV = GS >= 8 ? 3 : (GS == 4 ? 2 : 1);  // halving levels
   const int lane = threadIdx.x & 31;
   constexpr int CNT = 8 >> LV;                          // values a lane keeps after them
@@ -193,9 +237,10 @@ __device__ __forceinline__ double node_prs(const double* x, double gamma) {
 // its bounded re-limit loop, entropy-offset limiting, and the cell entropy.  x = this lane's node,
 // avg = the element average (all lanes of the group), node = lane's node (active = node < NN and
 // the group's element is limited).  Every lane of the warp calls this (the group reductions need
-// the whole warp); returns the cell entropy (0 where not computed) and sets *negcell.
+// the whole warp); returns the cell entropy (0 where not computed) and sets *negcell.  GS: lanes
+// per element of the caller's layout.
 // ---------------------------------------------------------------------------------------------
-template <int P>
+template <int P, int GS = PPCfg<P>::GS>
 __device__ __forceinline__ double limit_group(double* x, const double* avg, bool active, bool lead, int node,
                                               long long ce, const Geo& g, Ctrl* ctrl, int ent_offset,
                                               int comput_ent, const double* __restrict__ cell_ent_DG,
@@ -203,7 +248,7 @@ __device__ __forceinline__ double limit_group(double* x, const double* avg, bool
                                               const unsigned char* __restrict__ cell_ent_nan, bool* negcell,
                                               bool* scaled = nullptr) {
   using C = PPCfg<P>;
-  constexpr int N = C::N, GS = C::GS;
+  constexpr int N = C::N;
   constexpr double BIG = 1.7976931348623157e308;
   const double gamma = g.gamma;
   const DegConst& dc = c_deg[P];
@@ -382,7 +427,8 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   using C = PPCfg<P>;
   constexpr int N = C::N, NN = C::NN, EB = C::EB, N2 = C::N2, GS = C::GS, G = C::G, TE = C::TE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grp = lane / GS, node = lane - grp * GS;
+  const GrpLane<GS> gl = grp_lane<GS>();
+  const int grp = gl.grp, node = gl.node;
   const int nx = g.nx, ny = g.ny, NXG = nx + 2;
   const long long total = (long long)NXG * (ny + 2);
   const long long e0 = chunk * TE;
@@ -393,7 +439,7 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
   const double gamma = g.gamma;
   bool valid = false, inner = false;
   int i = 0, j = 0;
-  if (el < ne) {
+  if (el < ne && !gl.idle) {
     const GridRC me = grid_adv(cpos, el, NXG);  // cpos: the chunk's first element
     j = me.j;
     i = me.i;
@@ -922,16 +968,17 @@ __device__ __forceinline__ void pp_limit_segment(
     const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
     double* __restrict__ ent_out, double* __restrict__ accept_dst, int accept_only, double* s_ent, int* s_cnt) {
   using C = PPCfg<P>;
-  constexpr int NN = C::NN, EB = C::EB, GS = C::GS, G = C::G, TE = C::TE;
+  constexpr int NN = C::NN, EB = C::EB, GS = C::GSL, G = C::GL, TE = C::TEL;  // the limiter's groups
   if (ctrl->neg_avg) return;  // the reference skips loop 3 once neg_avg is set (DG_solver.f90:431)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grp = lane / GS, node = lane - grp * GS;
+  const GrpLane<GS> gl = grp_lane<GS>();
+  const int grp = gl.grp, node = gl.node;
   const int nx = g.nx, NXG = nx + 2;
   const int j = 1 + jrow;
   const int i0 = 1 + seg * TE;
   const int ne = min(TE, nx - i0 + 1);
   const int el = warp * G + grp;
-  const bool inside = el < ne, nd = node < NN;
+  const bool inside = el < ne && !gl.idle, nd = node < NN;
   const bool act = inside && nd;
   const long long e = (long long)j * NXG + i0 + el;
   const double gamma = g.gamma;
@@ -979,7 +1026,7 @@ __device__ __forceinline__ void pp_limit_segment(
       for (int v = 0; v < 8; ++v) x[v] = avg[v] + theta * (x[v] - avg[v]);
   }
   bool neg = false;
-  const double ce = limit_group<P>(x, avg, act, inside && node == 0, node, e, g, ctrl, ent_offset, comput_ent,
+  const double ce = limit_group<P, GS>(x, avg, act, inside && node == 0, node, e, g, ctrl, ent_offset, comput_ent,
                                    cell_ent_DG, cell_ent_FV, cell_ent_nan, &neg);
   const unsigned cnt = __popc(__ballot_sync(FULL_MASK, neg));
   if (lane == 0 && cnt) atomicAdd(s_cnt, (int)cnt);
@@ -1008,7 +1055,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
                     const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
                     const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
                     double* __restrict__ ent_partial, double* __restrict__ accept_dst, int accept_only) {
-  __shared__ double s_ent[PPCfg<P>::TE];
+  __shared__ double s_ent[PPCfg<P>::TEL];
   __shared__ int s_cnt;
   if (!gate_open(ctrl, gate)) return;
   if (threadIdx.x == 0) s_cnt = 0;
@@ -1028,7 +1075,7 @@ template <int P>
 __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
-  __shared__ double s_ent[PPCfg<P>::TE];
+  __shared__ double s_ent[PPCfg<P>::TEL];
   __shared__ int s_cnt;
   const int nw = *nwork, n = *ninst;
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
@@ -1037,7 +1084,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     if (!gate_open(d.ctrl, gate)) continue;
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
-    const int nseg = (d.g.nx + PPCfg<P>::TE - 1) / PPCfg<P>::TE;
+    const int nseg = (d.g.nx + PPCfg<P>::TEL - 1) / PPCfg<P>::TEL;
     const int seg = local % nseg, row = local / nseg;
     pp_limit_segment<P>(d.u[slot], d.u_avg, d.g, d.ctrl, seg, row, d.use_oedg && final, d.ctrl->dt,
                         d.ent_offset, final, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
