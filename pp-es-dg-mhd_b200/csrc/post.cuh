@@ -473,8 +473,18 @@ __device__ __forceinline__ void pp_avg_ldf_chunk(double* __restrict__ u, double*
     if (next_chunk >= 0) pp_prefetch<P>(u, g, next_chunk, npos, s1, bu, bk);
   } else if (s1.u0) {
     const double dts = __dmul_rn(s1.coef, *s1.dt);
+    if (inner && nd) {  // an interior node: u_con and k1 at this node (stage1_node's interior case)
+      const double* pu = s1.u0 + e * EB + node;
+      const double* pk = s1.k1 + ((long long)(j - 1) * nx + (i - 1)) * EB + node;
 #pragma unroll
-    for (int v = 0; v < 8; ++v) x[v] = act ? stage1_node<P>(s1, g, i, j, inner, v, node, dts) : 0.0;
+      for (int v = 0; v < 8; ++v) x[v] = __dadd_rn(pu[v * NN], __dmul_rn(dts, pk[v * NN]));
+    } else if (act) {  // a ghost element
+#pragma unroll
+      for (int v = 0; v < 8; ++v) x[v] = stage1_node<P>(s1, g, i, j, false, v, node, dts);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) x[v] = 0.0;
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < 8; ++v) x[v] = act ? u[e * EB + v * NN + node] : 0.0;
