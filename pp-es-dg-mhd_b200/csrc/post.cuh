@@ -1081,6 +1081,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
 
 // many instances: items = every member's row segments (row-major); the final stage applies OEDG
 // (if the instance uses it), computes the entropy and writes the accepted interior into slot 0
+// only, as the single-instance pipeline does
 template <int P>
 __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
@@ -1098,7 +1099,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
     const int seg = local % nseg, row = local / nseg;
     pp_limit_segment<P>(d.u[slot], d.u_avg, d.g, d.ctrl, seg, row, d.use_oedg && final, d.ctrl->dt,
                         d.ent_offset, final, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
-                        d.ent_partial + local, final ? d.u[0] : nullptr, 0, s_ent, &s_cnt);
+                        d.ent_partial + local, final ? d.u[0] : nullptr, final, s_ent, &s_cnt);
     __syncthreads();
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
@@ -1177,7 +1178,8 @@ __global__ void __launch_bounds__(256) stage_end_bc_batched(const InstDesc* __re
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
     const InstDesc& d = insts[it.m];
     if (*reinterpret_cast<volatile const int*>(&d.ctrl->state) != ST_RUN) continue;
-    bc_value<P>(d.u[slot], d.u[slot], d.g, (long long)it.local() * 256 + threadIdx.x);
+    // after the final stage the ring is filled from u_con, which alone holds the accepted interior
+    bc_value<P>(final ? d.u[0] : d.u[slot], d.u[slot], d.g, (long long)it.local() * 256 + threadIdx.x);
   }
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const InstDesc& d = insts[i];

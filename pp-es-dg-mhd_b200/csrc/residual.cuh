@@ -545,7 +545,9 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
     if (!gate_open(d.ctrl, gate)) continue;
     const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
     const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
-    if (!residual_tile2<P>(d.u[src], d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc))
+    // the state after the final stage: u_con's interior with the last stage array's ghost ring
+    const int srci = (src == d.R) ? 0 : src;
+    if (!residual_tile2<P>(d.u[srci], d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc))
       return;
     __syncthreads();  // the next tile reuses shared memory
   }
