@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
 // final-stage form (OEDG global reductions for instances that use OEDG); the other stages fuse
 // loop 3 (limit)
 template <int P, bool FINAL>
-__global__ void __launch_bounds__(PPCfg<P>::NT, FINAL ? (PPCfg<P>::MINB > 3 ? 3 : PPCfg<P>::MINB) : PPCfg<P>::MINB)
+__global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB > 3 ? 3 : PPCfg<P>::MINB)
     pp_avg_ldf_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                        const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int gate,
                        int stage1) {
@@ -1083,7 +1083,7 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
 // (if the instance uses it), computes the entropy and writes the accepted interior into slot 0
 // only, as the single-instance pipeline does
 template <int P>
-__global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
+__global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB > 3 ? 3 : PPCfg<P>::MINB)
     pp_limit_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   __shared__ double s_ent[PPCfg<P>::TEL];
