@@ -120,6 +120,7 @@ def test_launch_then_wait_equals_advance(pkg):
 FLAG_MIX = [  # (name, n, p, rknstg, use_oedg, use_ldf, ent_offset)
     ("blast", 16, 2, 3, 1, 1, 1), ("blast", 12, 2, 3, 0, 1, 0), ("ot2pi", 14, 3, 3, 1, 0, 0),
     ("rotor", 12, 1, 3, 0, 0, 1), ("ot2pi", 10, 2, 2, 1, 1, 1), ("rotor", 10, 3, 1, 1, 1, 0),
+    ("ot2pi", 12, 2, 5, 1, 1, 0),
 ]
 
 
@@ -160,7 +161,7 @@ def test_members_with_mixed_solve_flags_identical_to_solo_runs(pkg):
             m.close()
 
 
-@pytest.mark.parametrize("rknstg", [3, 2])
+@pytest.mark.parametrize("rknstg", [3, 2, 5])
 def test_batch_members_against_the_oracle(pkg, ora, rknstg):
     """each member of a mixed batch (degrees 1-3, different problems and meshes) against its own
     oracle run: the batched kernels themselves (residual2_batched, pp_*_batched,
