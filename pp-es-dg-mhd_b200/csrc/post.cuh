@@ -13,18 +13,19 @@
 //                       (DG_solver.f90:287-294) = max|u - g| = max(umax - g, g - umin) (rounding
 //                       is monotone), Zhang-Shu positivity
 //                       scaling with its bounded re-limit loop, entropy-offset limiting, cell
-//                       entropy (chunk partials, fixed order).
+//                       entropy (segment partials, fixed order); in the time-step pipeline the
+//                       final stage's result goes to u_con only (the accepted state).
 //   pp_entsum_kernel    total entropy from the partials (fixed order).
 //   stage_end_bc_kernel the end of a stage of the time-step pipeline in one launch: the entropy sum
 //                       (final stage), the stage-end decision, the next stage's pseudo-time and
 //                       the ghost fill of the stage state.
 //
-// Loops 1 and 3 work element-locally, so they map one element to a group of GS lanes of a warp,
-// one lane per GLL node, each lane holding its node's 8 variables in registers.  Loads and stores
-// of a variable are then 8*NN-byte runs per group (coalesced), per-element sums, minima and maxima
-// are butterfly reductions inside the group (every lane ends with the same value, since IEEE
-// addition, min and max are commutative), and no CTA-wide barrier sits between the steps of one
-// element.  A CTA of NT threads handles a chunk of TE = (NT/32) * (32/GS) consecutive
+// Loops 1 and 3 work element-locally, so they map one element to a group of lanes of a warp (GS
+// in loop 1, GSL in the limiter kernel; PPCfg), one lane per GLL node, each lane holding its node's
+// 8 variables in registers.  Loads and stores of a variable are then 8*NN-byte runs per group
+// (coalesced), per-element sums, minima and maxima are reductions inside the group (butterflies for
+// power-of-two groups, a fold plus a butterfly for the 9-lane groups; every lane ends with the same
+// value), and no CTA-wide barrier sits between the steps of one element.  A CTA of NT threads handles a chunk of TE = (NT/32) * (32/GS) consecutive
 // elements; per-chunk partial sums are formed in element order.  The single-instance loop-1
 // kernel is a persistent grid over the chunks in which each warp copies its elements of the next
 // chunk into shared memory (cp.async) while it works on the current one.  In the first stage of
