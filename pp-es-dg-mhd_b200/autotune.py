@@ -41,16 +41,16 @@ GROUPS = {
             3: [(4, 2, 128, 4), (4, 2, 128, 5), (4, 2, 128, 6), (8, 2, 256, 3)],
         },
     },
-    "post": {
+    "post": {  # sets 1 and 2 vary the indicator kernel, set 3 loops 1 and 3, against set 0
         "MHD_PP_CFG": {
-            1: [(256, 4), (128, 8), (256, 3), (192, 5)],
-            2: [(256, 4), (128, 8), (256, 3), (512, 2)],
-            3: [(256, 4), (128, 8), (256, 3), (192, 5)],
+            1: [(256, 4), (256, 4), (256, 4), (128, 8)],
+            2: [(256, 4), (256, 4), (256, 4), (128, 8)],
+            3: [(256, 4), (256, 4), (256, 4), (128, 8)],
         },
         "MHD_SIG_CFG": {
-            1: [(8, 8, 3), (8, 4, 4), (16, 4, 3), (4, 8, 4)],
-            2: [(8, 4, 3), (4, 4, 4), (8, 2, 3), (4, 8, 3)],
-            3: [(4, 4, 2), (4, 2, 3), (4, 3, 2), (2, 4, 3)],
+            1: [(8, 8, 3), (8, 8, 4), (8, 4, 4), (8, 8, 3)],
+            2: [(8, 4, 3), (8, 4, 4), (4, 4, 4), (8, 4, 3)],
+            3: [(4, 4, 2), (4, 4, 4), (4, 4, 3), (4, 4, 2)],
         },
     },
 }

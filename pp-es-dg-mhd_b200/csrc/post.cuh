@@ -812,6 +812,78 @@ __device__ __forceinline__ double sigsum_face(const double* Rp, const double* Lm
   return total;
 }
 
+// The part of sigsum_face from the normal-derivative orders KA and KB only (in that order): the two
+// halves {0, P} and {1, P-1} of a face at P = 3, each computed by its own warp (fewer registers,
+// half the dependent chain); the face's value is the sum of the two halves.
+template <int P, int KA, int KB>
+__device__ __forceinline__ double sigsum_face_pair(const double* Rp, const double* Lm, int sn, int st, double sn_h,
+                                                   double st_h, const double* coef) {
+  constexpr int N = P + 1;
+  const DegConst& dc = c_deg[P];
+  constexpr int KS[2] = {KA, KB};
+  double sk[2], J[2][N];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    double snk = 1.0;
+#pragma unroll
+    for (int i = 0; i < KS[h]; ++i) snk *= sn_h;  // sn_h^kk, the running product of sigsum_face
+    sk[h] = snk;
+  }
+#pragma unroll
+  for (int b = 0; b < N; ++b) {
+    double cr[N], cl[N];
+#pragma unroll
+    for (int a = 0; a < N; ++a) {
+      cr[a] = Rp[a * sn + b * st];
+      cl[a] = Lm[a * sn + b * st];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int kk = KS[h];
+      if (kk == 0) {
+        J[h][b] = cr[0] - cl[N - 1];
+      } else {
+        double tr = 0.0, tl = 0.0;
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+          tr += dc.R0[kk][a] * cr[a];
+          tl += dc.RN[kk][a] * cl[a];
+        }
+        J[h][b] = sk[h] * tr - sk[h] * tl;
+      }
+    }
+  }
+  double total = 0.0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int kk = KS[h];
+    double jump[N];
+#pragma unroll
+    for (int b = 0; b < N; ++b) jump[b] = J[h][b];
+#pragma unroll
+    for (int ll = 0; ll <= P; ++ll) {
+      if (ll > P - kk) break;
+      double L1 = 0.0;
+#pragma unroll
+      for (int b = 0; b < N; ++b) L1 += (0.5 * dc.qw[b]) * fabs(jump[b]);
+      total = total + coef[kk * N + ll] * L1;
+      if (ll < P - kk) {  // tangential derivative for the next order (D from the constant bank,
+        double nj[N];     // the scale applied after the sum: no scaled copy of D held in registers)
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+          double acc = 0.0;
+#pragma unroll
+          for (int b = 0; b < N; ++b) acc += dc.D[a + N * b] * jump[b];
+          nj[a] = st_h * acc;
+        }
+#pragma unroll
+        for (int a = 0; a < N; ++a) jump[a] = nj[a];
+      }
+    }
+  }
+  return total;
+}
+
 // coef[n][t] of sigsum_face for element size h (the reference's running products h^(n+t), n! t!)
 template <int P>
 __device__ __forceinline__ double sigsum_coef(int n, int t, double h) {
@@ -841,6 +913,7 @@ struct SigLayout {
   static constexpr int VS = NN + 1, ES = 8 * VS;   // padded variable / element record
   static constexpr int RW = TX + 2, RH = TY + 2;   // staged rectangle (max)
   static constexpr int DOUBLES = RW * RH * ES;
+  static constexpr int NQ = 8 * ((TX + 1) * TY + TX * (TY + 1));  // face-variable items of a tile, at most
 };
 
 
@@ -857,6 +930,7 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
   __shared__ double s_e[L::DOUBLES];  // face math reads its two variable blocks from here
   __shared__ double s_coef[2 * (P + 1) * (P + 1)];  // x faces (h = hx), then y faces (h = hy)
   __shared__ double s_mm[2][NT / 32][8];              // per warp: max, min of each variable
+  __shared__ double s_part[P == 3 ? 2 * L::NQ : 1];   // P = 3: the two halves of every item
   const int tid = threadIdx.x;
   const int nx = g.nx, ny = g.ny;
   const int i0 = 1 + tile_x * TX, j0 = 1 + tile_y * TY;
@@ -910,11 +984,10 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
   const double sxh = 2.0 / g.hx, syh = 2.0 / g.hy;
   const int wr = W + right, ht = H + top;  // TX and TY on interior tiles
   const int nfx = H * wr, nfy = W * ht;
-  for (int it = tid; it < 8 * (nfx + nfy); it += NT) {
-    const int v = it & 7, f = it >> 3;
-    const bool xf = f < nfx;
-    const double* lo;  // the element before the face
-    double* dst;
+  // face-variable item q: the variable's block of the element before the face, and the output
+  auto item = [&](int q, bool& xf, const double*& lo, double*& dst) {
+    const int v = q & 7, f = q >> 3;
+    xf = f < nfx;
     if (xf) {  // x face: row r, face c between columns c-1 and c of the tile
       const int r = (wr == TX) ? f / TX : f / wr, c = f - r * wr;
       lo = s_e + ((r + 1) * RW + c) * ES + v * VS;
@@ -925,9 +998,46 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
       lo = s_e + (r * RW + c + 1) * ES + v * VS;
       dst = sig_y + (((long long)(j0 + r - 1) * nx) + (i0 + c - 1)) * 8 + v;
     }
-    // one call site for both directions (the strides and scales select the direction)
-    *dst = sigsum_face<P>(lo + (xf ? ES : RW * ES), lo, xf ? 1 : P + 1, xf ? P + 1 : 1, xf ? sxh : syh,
-                          xf ? syh : sxh, s_coef + (xf ? 0 : (P + 1) * (P + 1)));
+  };
+  const int nq = 8 * (nfx + nfy);
+  if constexpr (P == 3) {
+    // two warps per 32 items: the even warps take the orders {0, 3}, the odd ones {1, 2}
+    // (sigsum_face_pair; the warp's half is uniform, so neither diverges); the halves meet in
+    // shared memory and are added in that order
+    static_assert(((NT / 32) & 1) == 0, "warps pair up");
+    for (int it = tid; it < 2 * ((nq + 31) & ~31); it += NT) {
+      const int half = (it >> 5) & 1, q = ((it >> 6) << 5) + (it & 31);
+      if (q < nq) {
+        bool xf;
+        const double* lo;
+        double* dst;
+        item(q, xf, lo, dst);
+        const double* rp = lo + (xf ? ES : RW * ES);
+        const int sn = xf ? 1 : P + 1, st = xf ? P + 1 : 1;
+        const double snh = xf ? sxh : syh, sth = xf ? syh : sxh;
+        const double* cf = s_coef + (xf ? 0 : (P + 1) * (P + 1));
+        s_part[half * L::NQ + q] = half == 0 ? sigsum_face_pair<P, 0, 3>(rp, lo, sn, st, snh, sth, cf)
+                                             : sigsum_face_pair<P, 1, 2>(rp, lo, sn, st, snh, sth, cf);
+      }
+    }
+    __syncthreads();
+    for (int q = tid; q < nq; q += NT) {
+      bool xf;
+      const double* lo;
+      double* dst;
+      item(q, xf, lo, dst);
+      *dst = s_part[q] + s_part[L::NQ + q];
+    }
+  } else {
+    for (int q = tid; q < nq; q += NT) {
+      bool xf;
+      const double* lo;
+      double* dst;
+      item(q, xf, lo, dst);
+      // one call site for both directions (the strides and scales select the direction)
+      *dst = sigsum_face<P>(lo + (xf ? ES : RW * ES), lo, xf ? 1 : P + 1, xf ? P + 1 : 1, xf ? sxh : syh,
+                            xf ? syh : sxh, s_coef + (xf ? 0 : (P + 1) * (P + 1)));
+    }
   }
   __syncthreads();
   if (tid < 16) {  // threads 0-7: max of variable tid; 8-15: min of variable tid - 8
