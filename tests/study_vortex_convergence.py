@@ -9,7 +9,10 @@ initial state again.  The errors are the reference's norms for its smooth test p
 over the eight conserved variables, and the max norm over nodes and variables.
 
     python tests/study_vortex_convergence.py [--meshes 64,128,256,512] [--degrees 1,2,3]
-                                             [--final-time 20] [--json out.json]
+                                             [--final-time 20] [--no-oedg] [--no-ldf] [--json out.json]
+
+--no-oedg / --no-ldf switch the OEDG damping / the LDF projection off (the discretisation's own
+order on a smooth solution, without the damping that dominates the error on coarse meshes).
 """
 import argparse
 import json
@@ -35,12 +38,12 @@ def errors(pkg, u, n, p, T, w):
     return l2, float(np.abs(d).max())
 
 
-def run(pkg, n, p, T):
+def run(pkg, n, p, T, oedg=True, ldf=True):
     prob = pkg.problems.make("vortex")
     t0 = time.perf_counter()
     with pkg.DGSolver.for_problem(prob, n, n, p) as g:
         g.init_problem(prob)
-        g.solve_begin(T, prob.cfl, True, True, False)
+        g.solve_begin(T, prob.cfl, oedg, ldf, False)
         st = g.advance(0, check_every=256)
         u = g.download_state(0)[:, :, :, 1:-1, 1:-1]
     wall = time.perf_counter() - t0
@@ -53,6 +56,8 @@ def main():
     ap.add_argument("--meshes", default="64,128,256,512")
     ap.add_argument("--degrees", default="1,2,3")
     ap.add_argument("--final-time", type=float, default=20.0)
+    ap.add_argument("--no-oedg", action="store_true")
+    ap.add_argument("--no-ldf", action="store_true")
     ap.add_argument("--json", default=None)
     a = ap.parse_args()
     import __graft_entry__
@@ -63,7 +68,7 @@ def main():
         w = pkg.problems.gll_nodes(p)[1]
         prev = None
         for n in meshes:
-            u, st, wall = run(pkg, n, p, a.final_time)
+            u, st, wall = run(pkg, n, p, a.final_time, not a.no_oedg, not a.no_ldf)
             l2, mx = errors(pkg, u, n, p, a.final_time, w)
             row = dict(p=p, n=n, steps=st["steps"], retries=st["retries"], l2=l2, max=mx, wall_s=wall)
             if prev:
