@@ -921,9 +921,17 @@ struct SigLayout {
 // into ctrl->umax_bits / umin_bits (order-preserving encodings; max and min are exact, so neither
 // the order of the merge nor the tiling changes the result).  The atomic is skipped when the value
 // already there is not exceeded, so that most tiles issue none.
+// Where the indicator tile's results go.  Taken by reference, so that the batched kernel can keep
+// it in shared memory instead of in registers for the whole tile.
+struct SigOut {
+  double* sig_x;
+  double* sig_y;
+  Ctrl* ctrl;
+};
+
 template <int P>
-__device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, Ctrl* ctrl, int tile_x,
-                                               int tile_y, double* __restrict__ sig_x, double* __restrict__ sig_y) {
+__device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, const Geo& g, const SigOut& so,
+                                               int tile_x, int tile_y) {
   using L = SigLayout<P>;
   constexpr int NN = L::NN, EB = L::EB, VS = L::VS, ES = L::ES, TX = L::TX, TY = L::TY, RW = L::RW;
   constexpr int NT = 256;
@@ -991,12 +999,12 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
     if (xf) {  // x face: row r, face c between columns c-1 and c of the tile
       const int r = (wr == TX) ? f / TX : f / wr, c = f - r * wr;
       lo = s_e + ((r + 1) * RW + c) * ES + v * VS;
-      dst = sig_x + (((long long)(j0 + r - 1) * (nx + 1)) + (i0 + c - 1)) * 8 + v;
+      dst = so.sig_x + (((long long)(j0 + r - 1) * (nx + 1)) + (i0 + c - 1)) * 8 + v;
     } else {  // y face: column c, face r between rows r-1 and r of the tile
       const int f2 = f - nfx;
       const int c = (ht == TY) ? f2 / TY : f2 / ht, r = f2 - c * ht;
       lo = s_e + (r * RW + c + 1) * ES + v * VS;
-      dst = sig_y + (((long long)(j0 + r - 1) * nx) + (i0 + c - 1)) * 8 + v;
+      dst = so.sig_y + (((long long)(j0 + r - 1) * nx) + (i0 + c - 1)) * 8 + v;
     }
   };
   const int nq = 8 * (nfx + nfy);
@@ -1044,7 +1052,7 @@ __device__ __forceinline__ void pp_sigsum_tile(const double* __restrict__ u, con
     const int v = tid & 7, lo = tid >> 3;
     double m = s_mm[lo][0][v];
     for (int w = 1; w < NT / 32; ++w) m = lo ? fmin(m, s_mm[1][w][v]) : fmax(m, s_mm[0][w][v]);
-    unsigned long long* dst = lo ? &ctrl->umin_bits[v] : &ctrl->umax_bits[v];
+    unsigned long long* dst = lo ? &so.ctrl->umin_bits[v] : &so.ctrl->umax_bits[v];
     const unsigned long long enc = ord_enc(m), cur = *reinterpret_cast<volatile unsigned long long*>(dst);
     if (lo ? (m < 1.0e308 && enc < cur) : (m > -1.0e308 && enc > cur)) {
       if (lo) atomicMin(dst, enc);
@@ -1058,7 +1066,7 @@ __global__ void __launch_bounds__(256, SigCfg<P>::MINB)
     pp_sigsum_kernel(const double* __restrict__ u, Geo g, Ctrl* ctrl, int gate,
                      double* __restrict__ sig_x, double* __restrict__ sig_y) {
   if (!gate_open(ctrl, gate)) return;
-  pp_sigsum_tile<P>(u, g, ctrl, blockIdx.x, blockIdx.y, sig_x, sig_y);
+  pp_sigsum_tile<P>(u, g, SigOut{sig_x, sig_y, ctrl}, blockIdx.x, blockIdx.y);
 }
 
 // many instances: items = every member's tiles (row-major)
@@ -1066,14 +1074,21 @@ template <int P>
 __global__ void __launch_bounds__(256, SigCfg<P>::MINB)
     pp_sigsum_batched(const InstDesc* __restrict__ insts, const int* __restrict__ pref,
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
+  __shared__ Geo s_g;  // the member's geometry and outputs, per tile (see SigOut)
+  __shared__ SigOut s_so;
   const int nw = *nwork, n = *ninst;
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
     const int m = it.m, local = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
+    if (threadIdx.x == 0) {
+      s_g = d.g;
+      s_so = SigOut{d.sig_x, d.sig_y, d.ctrl};
+    }
+    __syncthreads();
     const int ntx = (d.g.nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX;
-    pp_sigsum_tile<P>(d.u[slot], d.g, d.ctrl, local % ntx, local / ntx, d.sig_x, d.sig_y);
-    __syncthreads();  // the next tile reuses shared memory
+    pp_sigsum_tile<P>(d.u[slot], s_g, s_so, local % ntx, local / ntx);
+    __syncthreads();  // the next tile reuses shared memory (and s_g, s_so)
   }
 }
 
@@ -1081,16 +1096,29 @@ __global__ void __launch_bounds__(256, SigCfg<P>::MINB)
 // loop 3: OEDG damping, positivity, entropy offset, entropy.  A CTA owns TE consecutive
 // interior elements of one row j (a contiguous run of memory).
 // ---------------------------------------------------------------------------------------------
+// The arrays and switches of one limiter segment.  Taken by reference, so that the batched kernel
+// can keep them in shared memory (read where used) instead of in registers for the whole segment.
+struct LimitIO {
+  double* u;                  // the stage state (interior updated in place unless accept_only)
+  const double* u_avg;        // cell averages (loop 1)
+  Ctrl* ctrl;
+  const double* sig_x;        // OEDG face indicators (x faces, y faces)
+  const double* sig_y;
+  const double* cell_ent_DG;  // entropy-offset inputs of loop 1
+  const double* cell_ent_FV;
+  const unsigned char* cell_ent_nan;
+  double* ent_out;            // the segment's entropy partial (comput_ent)
+  double* accept_dst;         // the accepted state (u_con) or nullptr
+  double oedg_dt;
+  int apply_oedg, ent_offset, comput_ent, accept_only;
+};
+
 template <int P>
-__device__ __forceinline__ void pp_limit_segment(
-    double* __restrict__ u, const double* __restrict__ u_avg, const Geo& g, Ctrl* ctrl, int seg, int jrow,
-    int apply_oedg, double oedg_dt, int ent_offset, int comput_ent, const double* __restrict__ sig_x,
-    const double* __restrict__ sig_y, const double* __restrict__ cell_ent_DG,
-    const double* __restrict__ cell_ent_FV, const unsigned char* __restrict__ cell_ent_nan,
-    double* __restrict__ ent_out, double* __restrict__ accept_dst, int accept_only, double* s_ent, int* s_cnt) {
+__device__ __forceinline__ void pp_limit_segment(const LimitIO& io, const Geo& g, int seg, int jrow, double* s_ent,
+                                                 int* s_cnt) {
   using C = PPCfg<P>;
   constexpr int NN = C::NN, EB = C::EB, GS = C::GSL, G = C::GL, TE = C::TEL;  // the limiter's groups
-  if (ctrl->neg_avg) return;  // the reference skips loop 3 once neg_avg is set (DG_solver.f90:431)
+  if (io.ctrl->neg_avg) return;  // the reference skips loop 3 once neg_avg is set (DG_solver.f90:431)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const GrpLane<GS> gl = grp_lane<GS>();
   const int grp = gl.grp, node = gl.node;
@@ -1106,10 +1134,10 @@ __device__ __forceinline__ void pp_limit_segment(
   double x[8], avg[8];
 #pragma unroll
   for (int v = 0; v < 8; ++v) {
-    x[v] = act ? u[e * EB + v * NN + node] : 0.0;
-    avg[v] = inside ? u_avg[e * 8 + v] : 1.0;
+    x[v] = act ? io.u[e * EB + v * NN + node] : 0.0;
+    avg[v] = inside ? io.u_avg[e * 8 + v] : 1.0;
   }
-  if (apply_oedg) {  // DG_solver.f90:448-524
+  if (io.apply_oedg) {  // DG_solver.f90:448-524
     double sx = 0.0, sy = 0.0;
     if (act) {
       const double rho = fmax(x[0], PP_EPS);
@@ -1131,6 +1159,9 @@ __device__ __forceinline__ void pp_limit_segment(
       const long long fxl = ((long long)(j - 1) * (nx + 1) + (i - 1)) * 8;
       const long long fyb = ((long long)(j - 1) * nx + (i - 1)) * 8;
       const long long fyt = ((long long)j * nx + (i - 1)) * 8;
+      const Ctrl* ctrl = io.ctrl;
+      const double* sig_x = io.sig_x;
+      const double* sig_y = io.sig_y;
       for (int v = node; v < 8; v += GS) {
         const double gs = ctrl->u_avg_global[v];
         const double uv = fmax(0.0, fmax(ord_dec(ctrl->umax_bits[v]) - gs, gs - ord_dec(ctrl->umin_bits[v])));
@@ -1141,29 +1172,29 @@ __device__ __forceinline__ void pp_limit_segment(
       }
     }
     const double dmax = grp_max<GS>(d);
-    const double theta = exp(-oedg_dt * dmax);
+    const double theta = exp(-io.oedg_dt * dmax);
     if (act)
 #pragma unroll
       for (int v = 0; v < 8; ++v) x[v] = avg[v] + theta * (x[v] - avg[v]);
   }
   bool neg = false;
-  const double ce = limit_group<P, GS>(x, avg, act, inside && node == 0, node, e, g, ctrl, ent_offset, comput_ent,
-                                   cell_ent_DG, cell_ent_FV, cell_ent_nan, &neg);
+  const double ce = limit_group<P, GS>(x, avg, act, inside && node == 0, node, e, g, io.ctrl, io.ent_offset,
+                                       io.comput_ent, io.cell_ent_DG, io.cell_ent_FV, io.cell_ent_nan, &neg);
   const unsigned cnt = __popc(__ballot_sync(FULL_MASK, neg));
   if (lane == 0 && cnt) atomicAdd(s_cnt, (int)cnt);
   if (act)
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
-      if (!accept_only) u[e * EB + v * NN + node] = x[v];
-      if (accept_dst) accept_dst[e * EB + v * NN + node] = x[v];
+      if (!io.accept_only) io.u[e * EB + v * NN + node] = x[v];
+      if (io.accept_dst) io.accept_dst[e * EB + v * NN + node] = x[v];
     }
-  if (comput_ent) {  // chunk partial in element order
+  if (io.comput_ent) {  // chunk partial in element order
     if (inside && node == 0) s_ent[el] = ce;
     __syncthreads();
     if (tid == 0) {
       double tot = 0.0;
       for (int q = 0; q < ne; ++q) tot = tot + s_ent[q];
-      *ent_out = tot;
+      *io.ent_out = tot;
     }
   }
 }
@@ -1181,11 +1212,10 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB)
   if (!gate_open(ctrl, gate)) return;
   if (threadIdx.x == 0) s_cnt = 0;
   __syncthreads();
-  const double oedg_dt = dt_ptr ? *dt_ptr : oedg_dt_arg;
-  pp_limit_segment<P>(u, u_avg, g, ctrl, blockIdx.x, blockIdx.y, apply_oedg, oedg_dt, ent_offset, comput_ent,
-                      sig_x, sig_y, cell_ent_DG, cell_ent_FV, cell_ent_nan,
-                      ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst, accept_only, s_ent,
-                      &s_cnt);
+  const LimitIO io{u, u_avg, ctrl, sig_x, sig_y, cell_ent_DG, cell_ent_FV, cell_ent_nan,
+                   ent_partial + (long long)blockIdx.y * gridDim.x + blockIdx.x, accept_dst,
+                   dt_ptr ? *dt_ptr : oedg_dt_arg, apply_oedg, ent_offset, comput_ent, accept_only};
+  pp_limit_segment<P>(io, g, blockIdx.x, blockIdx.y, s_ent, &s_cnt);
   __syncthreads();
   if (threadIdx.x == 0 && s_cnt) atomicAdd(&ctrl->num_negcell, s_cnt);
 }
@@ -1199,18 +1229,24 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB > 3 ? 3 : PPCfg<P
                      const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   __shared__ double s_ent[PPCfg<P>::TEL];
   __shared__ int s_cnt;
+  __shared__ Geo s_g;      // the member's geometry and arrays, per item (see LimitIO)
+  __shared__ LimitIO s_io;
   const int nw = *nwork, n = *ninst;
   for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
     const int m = it.m, local = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
-    if (threadIdx.x == 0) s_cnt = 0;
+    if (threadIdx.x == 0) {
+      s_cnt = 0;
+      s_g = d.g;
+      s_io = LimitIO{d.u[slot], d.u_avg, d.ctrl, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
+                     d.ent_partial + local, final ? d.u[0] : nullptr, d.ctrl->dt, d.use_oedg && final,
+                     d.ent_offset, final, final};
+    }
     __syncthreads();
     const int nseg = (d.g.nx + PPCfg<P>::TEL - 1) / PPCfg<P>::TEL;
     const int seg = local % nseg, row = local / nseg;
-    pp_limit_segment<P>(d.u[slot], d.u_avg, d.g, d.ctrl, seg, row, d.use_oedg && final, d.ctrl->dt,
-                        d.ent_offset, final, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
-                        d.ent_partial + local, final ? d.u[0] : nullptr, final, s_ent, &s_cnt);
+    pp_limit_segment<P>(s_io, s_g, seg, row, s_ent, &s_cnt);
     __syncthreads();
     if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }

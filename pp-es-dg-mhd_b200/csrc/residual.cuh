@@ -132,6 +132,13 @@ __device__ __forceinline__ double group_max(double v, int gbase) {
   }
 }
 
+// Where a tile's results go: the L(u) array and the control block (dt_lim, flags).  Taken by
+// reference, so that the batched kernel can keep it in shared memory, out of the registers.
+struct TileOut {
+  double* ut;
+  Ctrl* ctrl;
+};
+
 // One tile (elements tile_x*TX + 1 .., tile_y*TY + 1 ..).  `phase` = the parity of the tile
 // barrier's next phase (flipped here).  Returns false if the wait for the tile's copies ran out
 // (FLAG_DEVICE_WAIT is then set): the caller must stop.  ug = the array whose ghost ring the
@@ -139,7 +146,7 @@ __device__ __forceinline__ double group_max(double v, int gbase) {
 // interior after the final stage; the interior always comes from u).
 template <int P>
 __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, const double* __restrict__ ug,
-                                               double* __restrict__ ut, const Geo& g, Ctrl* ctrl, int tile_x,
+                                               const TileOut& to, const Geo& g, int tile_x,
                                                int tile_y, double* sm, unsigned& phase,
                                                const StageCombine& sc = StageCombine{}) {
   using L = Res2Layout<P>;
@@ -214,7 +221,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, con
   {
     const bool ok = mbar_wait_bounded(bar, phase & 1u);
     if (__syncthreads_or(!ok)) {  // the copies did not arrive: flag it, give them one more bound, stop
-      if (tid == 0) atomicOr(&ctrl->flags, FLAG_DEVICE_WAIT);
+      if (tid == 0) atomicOr(&to.ctrl->flags, FLAG_DEVICE_WAIT);
       mbar_wait_bounded(bar, phase & 1u);
       __syncthreads();
       return false;
@@ -477,7 +484,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, con
         sc.out[e + v * NN] = __dadd_rn(__dmul_rn(sc.ca, u0n[v * NN]),
                                        __dmul_rn(sc.cb, __dadd_rn(w[v], __dmul_rn(dt, acc[v]))));
     } else {
-      double* o = ut + ((long long)(j0 + er - 1) * nx + (i0 + ec - 1)) * EB + node;
+      double* o = to.ut + ((long long)(j0 + er - 1) * nx + (i0 + ec - 1)) * EB + node;
 #pragma unroll
       for (int v = 0; v < 8; ++v) o[v * NN] = acc[v];
     }
@@ -491,7 +498,7 @@ __device__ __forceinline__ bool residual_tile2(const double* __restrict__ u, con
   if (tid == 0) {
     double m = s_red[0];
     for (int q = 1; q < NW; ++q) m = fmin(m, s_red[q]);
-    atomicMin(&ctrl->dt_lim_bits, (unsigned long long)__double_as_longlong(m));
+    atomicMin(&to.ctrl->dt_lim_bits, (unsigned long long)__double_as_longlong(m));
   }
   return true;
 }
@@ -505,7 +512,7 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
   extern __shared__ __align__(16) double sm[];
   res2_prologue<P>(sm);
   unsigned phase = 0;
-  residual_tile2<P>(u, ug, ut, g, ctrl, blockIdx.x, blockIdx.y, sm, phase, sc);
+  residual_tile2<P>(u, ug, TileOut{ut, ctrl}, g, blockIdx.x, blockIdx.y, sm, phase, sc);
 }
 
 // single instance, persistent: CTA b computes tiles b, b + gridDim.x, ... (row-major, ntx per row).
@@ -520,7 +527,7 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
   res2_prologue<P>(sm);
   unsigned phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    if (!residual_tile2<P>(u, u, ut, g, ctrl, t % ntx, t / ntx, sm, phase, StageCombine{})) return;
+    if (!residual_tile2<P>(u, u, TileOut{ut, ctrl}, g, t % ntx, t / ntx, sm, phase, StageCombine{})) return;
     __syncthreads();  // the next tile reuses shared memory
   }
 }
@@ -536,6 +543,12 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int src, int dst, int gate,
                       int next_stage, double ca, double cb) {
   extern __shared__ __align__(16) double sm[];
+  // the member's geometry, stage combination and outputs, copied per tile into shared memory: the
+  // tile reads them there after each barrier instead of holding them in registers from the table
+  // entry (the single-instance kernel reads them from its parameters in the same way)
+  __shared__ Geo s_g;
+  __shared__ StageCombine s_sc;
+  __shared__ TileOut s_to;
   res2_prologue<P>(sm);
   unsigned phase = 0;
   const int nw = *nwork, n = *ninst;
@@ -543,13 +556,18 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
     const int m = it.m, local = it.local();
     const InstDesc& d = insts[m];
     if (!gate_open(d.ctrl, gate)) continue;
+    if (threadIdx.x == 0) {
+      s_g = d.g;
+      s_sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
+      s_to = TileOut{d.ut[dst], d.ctrl};
+    }
+    __syncthreads();
     const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
-    const StageCombine sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
     // the state after the final stage: u_con's interior with the last stage array's ghost ring
     const int srci = (src == d.R) ? 0 : src;
-    if (!residual_tile2<P>(d.u[srci], d.u[src], d.ut[dst], d.g, d.ctrl, local % ntx, local / ntx, sm, phase, sc))
+    if (!residual_tile2<P>(d.u[srci], d.u[src], s_to, s_g, local % ntx, local / ntx, sm, phase, s_sc))
       return;
-    __syncthreads();  // the next tile reuses shared memory
+    __syncthreads();  // the next tile reuses shared memory (and s_g, s_sc, s_to)
   }
 }
 
