@@ -177,6 +177,28 @@ struct BatchWalk {
   }
 };
 
+// BatchWalk's order of items with the walker's state in shared memory, for kernels whose items need
+// every register: thread 0 starts and advances it, between barriers of the whole CTA.
+struct SharedWalk {
+  int w, last, m, mstart, mend;
+  __device__ __forceinline__ void start(const int* __restrict__ pref, int n, int nw) {
+    const BatchWalk it(pref, n, nw);
+    w = it.w;
+    last = it.last;
+    m = it.m;
+    mstart = it.mstart;
+    mend = it.mend;
+  }
+  __device__ __forceinline__ void advance(const int* __restrict__ pref) {
+    ++w;
+    while (w < last && w >= mend) {
+      ++m;
+      mstart = mend;
+      mend = __ldg(pref + m + 1);
+    }
+  }
+};
+
 // ---- order-preserving encodings of doubles for atomicMax / atomicMin --------------------------
 __device__ __forceinline__ unsigned long long ord_enc(double x) {
   long long b = __double_as_longlong(x);

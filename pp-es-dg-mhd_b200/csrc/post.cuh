@@ -666,28 +666,33 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB > 3 ? 3 : PPCfg<P
   __shared__ __align__(16) double s_ldf[C::TE * (C::N2 + 2)];
   __shared__ double s_red[C::TE * 8];  // chunk sums (the loop's barriers protect it)
   __shared__ int s_cnt;
-  const int nw = *nwork, n = *ninst;
+  __shared__ SharedWalk s_walk;  // the walker's state, out of the registers the chunk needs
+  if (threadIdx.x == 0) s_walk.start(pref, *ninst, *nwork);
+  __syncthreads();
   int loaded = -1;  // member whose LDF operator s_A holds
-  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
-    const int m = it.m, chunk = it.local();
+  while (s_walk.w < s_walk.last) {
+    const int m = s_walk.m, chunk = s_walk.w - s_walk.mstart;
     const InstDesc& d = insts[m];
-    if (!gate_open(d.ctrl, gate)) continue;
-    if (threadIdx.x == 0) s_cnt = 0;
-    if (d.use_ldf && loaded != m) {
-      __syncthreads();
-      load_ldf<P>(d.g.ldfA, s_A);
-      loaded = m;
+    const bool open = gate_open(d.ctrl, gate);
+    if (open) {
+      if (d.use_ldf && loaded != m) {  // (the previous item ended with a barrier)
+        load_ldf<P>(d.g.ldfA, s_A);
+        loaded = m;
+      }
+      if (threadIdx.x == 0) s_cnt = 0;
     }
-    __syncthreads();
-    const int need_global = FINAL && d.use_oedg;
-    const Stage1Src s1 = stage1 ? Stage1Src{d.u[0], d.ut[1], &d.ctrl->dt, stage1_coef(d.R)} : Stage1Src{};
-    pp_avg_ldf_chunk<P, FINAL, false>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk,
-                                      grid_rc((long long)chunk * C::TE, d.g.nx + 2), d.use_ldf, need_global,
-                                      d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
-                                      d.cell_ent_nan, !FINAL, s_A, s_ldf, s_red, &s_cnt, s1,
-                                      nullptr, nullptr, -1, GridRC{0, 0});
-    __syncthreads();
-    if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
+    __syncthreads();  // every thread has read the walker; s_A and s_cnt are in place
+    if (threadIdx.x == 0) s_walk.advance(pref);
+    if (open) {
+      const Stage1Src s1 = stage1 ? Stage1Src{d.u[0], d.ut[1], &d.ctrl->dt, stage1_coef(d.R)} : Stage1Src{};
+      pp_avg_ldf_chunk<P, FINAL, false>(d.u[slot], d.u_avg, d.g, d.ctrl, chunk,
+                                        grid_rc((long long)chunk * C::TE, d.g.nx + 2), d.use_ldf, FINAL && d.use_oedg,
+                                        d.ent_offset, d.partial + (long long)chunk * 8, d.cell_ent_DG, d.cell_ent_FV,
+                                        d.cell_ent_nan, !FINAL, s_A, s_ldf, s_red, &s_cnt, s1,
+                                        nullptr, nullptr, -1, GridRC{0, 0});
+    }
+    __syncthreads();  // the item is done; the walker has advanced
+    if (open && threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
   }
 }
 
@@ -1076,19 +1081,24 @@ __global__ void __launch_bounds__(256, SigCfg<P>::MINB)
                       const int* __restrict__ nwork, const int* __restrict__ ninst, int slot, int final, int gate) {
   __shared__ Geo s_g;  // the member's geometry and outputs, per tile (see SigOut)
   __shared__ SigOut s_so;
-  const int nw = *nwork, n = *ninst;
-  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
-    const int m = it.m, local = it.local();
+  __shared__ SharedWalk s_walk;
+  if (threadIdx.x == 0) s_walk.start(pref, *ninst, *nwork);
+  __syncthreads();
+  while (s_walk.w < s_walk.last) {
+    const int m = s_walk.m, local = s_walk.w - s_walk.mstart;
     const InstDesc& d = insts[m];
-    if (!gate_open(d.ctrl, gate) || !(d.use_oedg && final)) continue;
-    if (threadIdx.x == 0) {
+    const bool open = gate_open(d.ctrl, gate) && d.use_oedg && final;
+    if (open && threadIdx.x == 0) {
       s_g = d.g;
       s_so = SigOut{d.sig_x, d.sig_y, d.ctrl};
     }
-    __syncthreads();
-    const int ntx = (d.g.nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX;
-    pp_sigsum_tile<P>(d.u[slot], s_g, s_so, local % ntx, local / ntx);
-    __syncthreads();  // the next tile reuses shared memory (and s_g, s_so)
+    __syncthreads();  // every thread has read the walker; the item's arguments are in place
+    if (threadIdx.x == 0) s_walk.advance(pref);
+    if (open) {
+      const int ntx = (d.g.nx + SigCfg<P>::TX - 1) / SigCfg<P>::TX;
+      pp_sigsum_tile<P>(d.u[slot], s_g, s_so, local % ntx, local / ntx);
+    }
+    __syncthreads();  // the item is done (the next one reuses shared memory); the walker has advanced
   }
 }
 
@@ -1231,24 +1241,28 @@ __global__ void __launch_bounds__(PPCfg<P>::NT, PPCfg<P>::MINB > 3 ? 3 : PPCfg<P
   __shared__ int s_cnt;
   __shared__ Geo s_g;      // the member's geometry and arrays, per item (see LimitIO)
   __shared__ LimitIO s_io;
-  const int nw = *nwork, n = *ninst;
-  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
-    const int m = it.m, local = it.local();
+  __shared__ SharedWalk s_walk;
+  if (threadIdx.x == 0) s_walk.start(pref, *ninst, *nwork);
+  __syncthreads();
+  while (s_walk.w < s_walk.last) {
+    const int m = s_walk.m, local = s_walk.w - s_walk.mstart;
     const InstDesc& d = insts[m];
-    if (!gate_open(d.ctrl, gate)) continue;
-    if (threadIdx.x == 0) {
+    const bool open = gate_open(d.ctrl, gate);
+    if (open && threadIdx.x == 0) {
       s_cnt = 0;
       s_g = d.g;
       s_io = LimitIO{d.u[slot], d.u_avg, d.ctrl, d.sig_x, d.sig_y, d.cell_ent_DG, d.cell_ent_FV, d.cell_ent_nan,
                      d.ent_partial + local, final ? d.u[0] : nullptr, d.ctrl->dt, d.use_oedg && final,
                      d.ent_offset, final, final};
     }
-    __syncthreads();
-    const int nseg = (d.g.nx + PPCfg<P>::TEL - 1) / PPCfg<P>::TEL;
-    const int seg = local % nseg, row = local / nseg;
-    pp_limit_segment<P>(s_io, s_g, seg, row, s_ent, &s_cnt);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_cnt) atomicAdd(&d.ctrl->num_negcell, s_cnt);
+    __syncthreads();  // every thread has read the walker; the item's arguments are in place
+    if (threadIdx.x == 0) s_walk.advance(pref);
+    if (open) {
+      const int nseg = (d.g.nx + PPCfg<P>::TEL - 1) / PPCfg<P>::TEL;
+      pp_limit_segment<P>(s_io, s_g, local % nseg, local / nseg, s_ent, &s_cnt);
+    }
+    __syncthreads();  // the item is done; the walker has advanced
+    if (open && threadIdx.x == 0 && s_cnt) atomicAdd(&s_io.ctrl->num_negcell, s_cnt);
   }
 }
 

@@ -549,25 +549,29 @@ __global__ void __launch_bounds__(Res2Cfg<P>::NT, Res2Cfg<P>::MINB)
   __shared__ Geo s_g;
   __shared__ StageCombine s_sc;
   __shared__ TileOut s_to;
-  res2_prologue<P>(sm);
+  __shared__ SharedWalk s_walk;  // the walker's state, out of the registers the tile needs
+  if (threadIdx.x == 0) s_walk.start(pref, *ninst, *nwork);
+  res2_prologue<P>(sm);  // (ends with a barrier)
   unsigned phase = 0;
-  const int nw = *nwork, n = *ninst;
-  for (BatchWalk it(pref, n, nw); it.more(); it.next()) {
-    const int m = it.m, local = it.local();
+  while (s_walk.w < s_walk.last) {
+    const int m = s_walk.m, local = s_walk.w - s_walk.mstart;
     const InstDesc& d = insts[m];
-    if (!gate_open(d.ctrl, gate)) continue;
-    if (threadIdx.x == 0) {
+    const bool open = gate_open(d.ctrl, gate);
+    if (open && threadIdx.x == 0) {
       s_g = d.g;
       s_sc = next_stage > 0 ? StageCombine{d.u[0], d.u[next_stage], ca, cb, &d.ctrl->dt} : StageCombine{};
       s_to = TileOut{d.ut[dst], d.ctrl};
     }
-    __syncthreads();
-    const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
-    // the state after the final stage: u_con's interior with the last stage array's ghost ring
-    const int srci = (src == d.R) ? 0 : src;
-    if (!residual_tile2<P>(d.u[srci], d.u[src], s_to, s_g, local % ntx, local / ntx, sm, phase, s_sc))
-      return;
-    __syncthreads();  // the next tile reuses shared memory (and s_g, s_sc, s_to)
+    __syncthreads();  // every thread has read the walker; the item's arguments are in place
+    if (threadIdx.x == 0) s_walk.advance(pref);
+    if (open) {
+      const int ntx = (d.g.nx + Res2Cfg<P>::TX - 1) / Res2Cfg<P>::TX;
+      // the state after the final stage: u_con's interior with the last stage array's ghost ring
+      const int srci = (src == d.R) ? 0 : src;
+      if (!residual_tile2<P>(d.u[srci], d.u[src], s_to, s_g, local % ntx, local / ntx, sm, phase, s_sc))
+        return;
+    }
+    __syncthreads();  // the item is done (the next one reuses shared memory); the walker has advanced
   }
 }
 
