@@ -2,7 +2,7 @@
 
 Tolerances (FP64):
   * residual ut, post-processed states, one SSP-RK3 step: relative L1 per conserved variable
-    <= 1e-12 (the north-star parity bar; observed differences are at the 1e-15 level, from FMA
+    <= 1e-12 (the one-step parity bar; observed differences are at the 1e-15 level, from FMA
     contraction and libm vs CUDA log/exp/sqrt rounding);
   * dt_lim, tot_ent: relative 1e-13;
   * integer outputs (neg_avg, num_negcell, retries, steps): exact.
