@@ -6,8 +6,8 @@ module advected with velocity (1, 1) on [-10, 10]^2, periodic, against its exact
 the momentum and field components:
 
   * OEDG off (LDF and the positivity limiter on, neither active on this smooth flow): order
-    >= p + 0.6 for p = 1, 2, 3 on 32^2 -> 64^2 (the oracle gives 1.9, 2.9, 4.1);
-  * OEDG on: order >= p + 0.6 for p = 1, 2 on 64^2 -> 128^2 (the oracle gives 2.1, 3.8).  At p = 3
+    >= p + 0.6 for p = 1, 2, 3 on 32^2 -> 64^2 (the oracle gives 1.8, 2.9, 4.1);
+  * OEDG on: order >= p + 0.6 for p = 1, 2 on 64^2 -> 128^2 (the oracle gives 2.1, 3.9).  At p = 3
     these meshes are still pre-asymptotic for the damping (the oracle gives 1.1 on 32^2 -> 64^2),
     so p = 3 with OEDG is not asserted here.
 """
