@@ -1,6 +1,6 @@
 """The commands the ncu summaries under profiles/ give still run committed files (CPU).
 
-Every `python <script> ...` command quoted in a profiles/*.md summary must name a script of this
+Every `python <script> ...` command quoted in one of those summaries must name a script of this
 repository, and every `--option` it passes must be one that script defines, so that a reader can
 re-run the command that made the figures.
 """
